@@ -1,0 +1,163 @@
+"""gpufft_b200 — Python mirror of GPU-FFT's polynomial-multiplication API.
+
+The names, argument order and error behaviour follow the reference's C++ API
+(src/include/gpufft/fft.cuh:37-51, 120-132, 269-273; src/lib/fft.cu:517-725,
+1386-1515):
+
+* ``fft_configuration`` (n_power, fft_type, reduction_poly, zero_padding,
+  mod_inverse, stream), ``FORWARD``/``INVERSE``, ``X_N_plus``/``X_N_minus``;
+* ``GPU_FFT(inout, roots, cfg, batch, multiplication)`` (C_C) and
+  ``GPU_FFT(real_inout, temp, roots, cfg, batch, multiplication)`` (R_R);
+* ``GPU_FFNT(inout, temp, twist_or_untwist, roots, cfg, batch, multiplication)``;
+* ``ValueError("Invalid n_power range!")`` where the reference throws
+  ``std::invalid_argument`` and ``CudaException`` where it throws one.
+
+Every call goes through the C ABI of ``lib/libgpufft_b200.so`` (declared in
+``include/gpufft_b200.h``) on hand-written sm_100a kernels. Device buffers are
+torch CUDA tensors, used only for memory and streams. There is no CPU
+fallback: importing this package without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Optional
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgpufft_b200.so")
+
+FORWARD, INVERSE = 0, 1
+X_N_plus, X_N_minus = 0, 1
+
+SUCCESS = 0
+ERROR_INVALID_N_POWER = 1
+ERROR_INVALID_VALUE = 2
+ERROR_CUDA = 3
+ERROR_WORKSPACE = 4
+ERROR_MISALIGNED = 5
+
+
+class CudaException(RuntimeError):
+    """A CUDA error raised under a library call (reference common_fft.cuh:19-49)."""
+
+    def __init__(self, where: str, code: int):
+        self.code = code
+        super().__init__(f"CUDA Error in {where}: cudaError {code}")
+
+
+class GpufftError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        self.status = status
+        super().__init__(msg)
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the native library; raise if it was not built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"gpufft_b200 native library missing: {LIB_PATH} (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, f, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
+        L.gpufft_fft_c2c_f32.argtypes = [vp, vp, i, i, i, i, f, f, i, i, vp]
+        L.gpufft_fft_c2c_f64.argtypes = [vp, vp, i, i, i, i, d, d, i, i, vp]
+        L.gpufft_fft_r2r_f32.argtypes = [vp, vp, vp, i, i, i, i, f, f, i, i, vp]
+        L.gpufft_fft_r2r_f64.argtypes = [vp, vp, vp, i, i, i, i, d, d, i, i, vp]
+        L.gpufft_ffnt_f32.argtypes = [vp, vp, vp, vp, i, i, f, f, i, i, vp]
+        L.gpufft_ffnt_f64.argtypes = [vp, vp, vp, vp, i, i, d, d, i, i, vp]
+        L.gpufft_last_cuda_error.restype = i
+        L.gpufft_status_string.restype = ctypes.c_char_p
+        L.gpufft_status_string.argtypes = [i]
+        L.gpufft_version.restype = i
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    """Map a C-ABI status to the reference's exceptions."""
+    if status == SUCCESS:
+        return
+    if status == ERROR_INVALID_N_POWER:
+        raise ValueError("Invalid n_power range!")
+    if status == ERROR_CUDA:
+        raise CudaException(where, lib().gpufft_last_cuda_error())
+    raise GpufftError(status, f"{where}: {lib().gpufft_status_string(status).decode()}")
+
+
+@dataclasses.dataclass
+class fft_configuration:
+    """gpufft::fft_configuration<T> (reference fft.cuh:43-51)."""
+    n_power: int = 0
+    fft_type: int = FORWARD
+    reduction_poly: int = X_N_minus
+    zero_padding: bool = False
+    mod_inverse: complex = 1.0 + 0.0j
+    stream: Optional[object] = None  # torch.cuda.Stream, a raw cudaStream_t int, or None
+
+
+def _stream_handle(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream or None
+    if isinstance(stream, int):
+        return stream or None
+    return stream.cuda_stream or None
+
+
+def _ptr(t) -> int:
+    if not t.is_cuda:
+        raise GpufftError(ERROR_INVALID_VALUE, "device buffers must be CUDA tensors")
+    return t.data_ptr()
+
+
+def _is_f64(t) -> bool:
+    import torch
+    return t.dtype in (torch.float64, torch.complex128)
+
+
+def _range_check(n_power: int) -> None:
+    # reference fft.cu:522-525, 606-609, 1392-1395
+    if n_power <= 11 or n_power >= 25:
+        raise ValueError("Invalid n_power range!")
+
+
+def GPU_FFT(*args):
+    """GPU_FFT(inout, roots, cfg, batch, multiplication)            -- C_C
+    GPU_FFT(real_inout, temp, roots, cfg, batch, multiplication)     -- R_R
+    (reference fft.cuh:120-132)."""
+    L = lib()
+    if len(args) == 5:
+        inout, roots, cfg, batch, mult = args
+        _range_check(cfg.n_power)
+        f = L.gpufft_fft_c2c_f64 if _is_f64(inout) else L.gpufft_fft_c2c_f32
+        st = f(_ptr(inout), _ptr(roots), cfg.n_power, int(cfg.fft_type), int(cfg.reduction_poly),
+               int(bool(cfg.zero_padding)), complex(cfg.mod_inverse).real, complex(cfg.mod_inverse).imag,
+               int(batch), int(bool(mult)), _stream_handle(cfg.stream))
+        check(st, "GPU_FFT")
+        return
+    if len(args) == 6:
+        real_inout, temp, roots, cfg, batch, mult = args
+        _range_check(cfg.n_power)
+        f = L.gpufft_fft_r2r_f64 if _is_f64(real_inout) else L.gpufft_fft_r2r_f32
+        st = f(_ptr(real_inout), _ptr(temp), _ptr(roots), cfg.n_power, int(cfg.fft_type),
+               int(cfg.reduction_poly), int(bool(cfg.zero_padding)), complex(cfg.mod_inverse).real,
+               complex(cfg.mod_inverse).imag, int(batch), int(bool(mult)), _stream_handle(cfg.stream))
+        check(st, "GPU_FFT")
+        return
+    raise TypeError("GPU_FFT takes 5 (C_C) or 6 (R_R) arguments")
+
+
+def GPU_FFNT(inout, temp, twist_table, root_table, cfg, batch, multiplication):
+    """GPU_FFNT (reference fft.cuh:269-273, fft.cu:1386-1515). For the inverse,
+    pass the untwist table as twist_table, as the reference's callers do."""
+    _range_check(cfg.n_power)
+    L = lib()
+    f = L.gpufft_ffnt_f64 if _is_f64(inout) else L.gpufft_ffnt_f32
+    st = f(_ptr(inout), _ptr(temp), _ptr(twist_table), _ptr(root_table), cfg.n_power, int(cfg.fft_type),
+           complex(cfg.mod_inverse).real, complex(cfg.mod_inverse).imag, int(batch), int(bool(multiplication)),
+           _stream_handle(cfg.stream))
+    check(st, "GPU_FFNT")

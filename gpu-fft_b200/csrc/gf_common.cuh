@@ -1,0 +1,95 @@
+// gpufft-b200: shared device/host helpers for the sm_100a kernels.
+//
+// Complex values use the reference's COMPLEX<T> layout (complex.cuh:28-34):
+// a float2 / double2 with the real part first. The arithmetic below keeps the
+// reference's expression shapes (complex.cuh:65-69 add, 99-104 sub, 133-139
+// mul) so that the compiler contracts them to FMA the same way it does for
+// the reference kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/gpufft_b200.h"
+
+namespace gfb
+{
+
+template <typename T> struct vec2_of;
+template <> struct vec2_of<float> { using type = float2; };
+template <> struct vec2_of<double> { using type = double2; };
+template <typename T> using cx = typename vec2_of<T>::type;
+
+template <typename T> __host__ __device__ __forceinline__ cx<T> mk(T r, T i)
+{
+    cx<T> c;
+    c.x = r;
+    c.y = i;
+    return c;
+}
+template <typename T> __device__ __forceinline__ cx<T> cadd(cx<T> a, cx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __device__ __forceinline__ cx<T> csub(cx<T> a, cx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b)
+{
+    return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <typename T> __device__ __forceinline__ cx<T> cmulc(cx<T> a, cx<T> b)
+{
+    return mk<T>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// Radix-2 butterflies, the two units of fft.cuh:69-89.
+template <typename T> __device__ __forceinline__ void ct_bfly(cx<T>& U, cx<T>& V, cx<T> w)
+{
+    cx<T> u = U;
+    cx<T> v = cmul<T>(V, w);
+    U = cadd<T>(u, v);
+    V = csub<T>(u, v);
+}
+template <typename T> __device__ __forceinline__ void gs_bfly(cx<T>& U, cx<T>& V, cx<T> w)
+{
+    cx<T> u = U;
+    cx<T> v = V;
+    U = cadd<T>(u, v);
+    V = cmul<T>(csub<T>(u, v), w);
+}
+
+// Read-only loads through the non-coherent path; streaming loads and stores
+// for data touched once (evict-first in L2 so that twiddle tables and
+// inter-pass spectra stay resident).
+template <typename T> __device__ __forceinline__ cx<T> ldg(const cx<T>* p) { return __ldg(p); }
+template <typename T> __device__ __forceinline__ T ldg_s(const T* p) { return __ldg(p); }
+template <typename V> __device__ __forceinline__ V ld_stream(const V* p) { return __ldcs(p); }
+template <typename V> __device__ __forceinline__ void st_stream(V* p, V v) { __stcs(p, v); }
+
+} // namespace gfb
+
+// Host-side status plumbing shared by every entry point.
+namespace gfb
+{
+int set_cuda_error(cudaError_t e);
+int check_launch();
+
+// Opt a kernel into more than 48 KB of dynamic shared memory, once per device.
+template <typename K> int ensure_smem(K* kernel, size_t bytes)
+{
+    static int done[64] = {0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    if (dev < 0 || dev >= 64) return set_cuda_error(cudaErrorInvalidDevice);
+    if (done[dev] >= (int)bytes) return 0;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    done[dev] = (int)bytes;
+    return 0;
+}
+} // namespace gfb
+
+#define GFB_TRY_CUDA(expr)                                                                       \
+    do                                                                                           \
+    {                                                                                            \
+        cudaError_t _e = (expr);                                                                 \
+        if (_e != cudaSuccess) return gfb::set_cuda_error(_e);                                   \
+    } while (0)

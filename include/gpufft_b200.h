@@ -1,0 +1,119 @@
+/*
+ * gpufft-b200 — C ABI of the B200 (sm_100a) polynomial-multiplication library.
+ *
+ * Every function returns a gpufft_status code (0 = success). Pointers are
+ * device pointers owned by the caller unless a comment says otherwise; the
+ * library keeps no per-call state. Work is enqueued asynchronously on
+ * `stream` (a cudaStream_t; NULL is the legacy default stream), exactly as the
+ * reference's GPU_FFT / GPU_FFNT enqueue on cfg.stream and never synchronize
+ * (reference src/lib/fft.cu:517-725, 1386-1515).
+ *
+ * Complex buffers use the reference's COMPLEX<T> layout: interleaved
+ * (re, im) float2 / double2 (reference src/include/gpufft/complex.cuh:28-34,
+ * 315-318).
+ */
+#ifndef GPUFFT_B200_H
+#define GPUFFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* gpufft_stream_t; /* identical to cudaStream_t */
+
+enum gpufft_status
+{
+    GPUFFT_SUCCESS = 0,
+    /* n_power outside the supported range; the C++ drop-in maps this to
+     * std::invalid_argument("Invalid n_power range!") (reference fft.cu:522-525) */
+    GPUFFT_ERROR_INVALID_N_POWER = 1,
+    /* a null pointer, a non-positive batch, an unknown enum value, or a size
+     * whose element count does not fit the kernels' 64-bit indexing */
+    GPUFFT_ERROR_INVALID_VALUE = 2,
+    /* a CUDA call or kernel launch failed: gpufft_last_cuda_error() holds the
+     * cudaError_t, which the C++ drop-in rethrows as gpufft::CudaException
+     * (reference common_fft.cuh:19-49) */
+    GPUFFT_ERROR_CUDA = 3,
+    /* the caller's workspace is smaller than the *_workspace_bytes query */
+    GPUFFT_ERROR_WORKSPACE = 4,
+    /* a device pointer is not aligned to its element type (8/16 bytes) */
+    GPUFFT_ERROR_MISALIGNED = 5
+};
+
+/* gpufft::type (reference fft.cuh:37-41) */
+enum { GPUFFT_FORWARD = 0, GPUFFT_INVERSE = 1 };
+/* gpufft::ReductionPolynomial (reference fft_cpu.cuh:69-73) */
+enum { GPUFFT_X_N_PLUS = 0, GPUFFT_X_N_MINUS = 1 };
+
+/* The cudaError_t of the last GPUFFT_ERROR_CUDA raised on this host thread. */
+int gpufft_last_cuda_error(void);
+/* A static, human-readable string for a gpufft_status value. */
+const char* gpufft_status_string(int status);
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int gpufft_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in transforms (the reference's GPU_FFT / GPU_FFNT, same arguments).  */
+/* n_power is accepted in [1, 24] for the FFT and [2, 25] for the FFNT; the  */
+/* C++ and Python drop-in layers add the reference's [12, 24] check.         */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces GPU_FFT(COMPLEX<T>* device_inout, COMPLEX<T>* root_of_unity_table,
+ * fft_configuration<T> cfg, int batch_size, bool multiplication)
+ * — reference fft.cuh:120-124, fft.cu:517-598.
+ * Forward: `batch` in-place transforms of 2^n_power complex values, natural
+ * order in, +sign DFT in bit-reversed order out. Inverse: with multiplication
+ * the operand is inout[i] * inout[i + batch*2^n_power]; the result (scaled by
+ * mod_inverse) overwrites the first `batch` vectors. */
+int gpufft_fft_c2c_f32(void* inout, const void* root_table, int n_power, int fft_type,
+                       int reduction_poly, int zero_padding, float mod_inverse_re,
+                       float mod_inverse_im, int batch, int multiplication, gpufft_stream_t stream);
+int gpufft_fft_c2c_f64(void* inout, const void* root_table, int n_power, int fft_type,
+                       int reduction_poly, int zero_padding, double mod_inverse_re,
+                       double mod_inverse_im, int batch, int multiplication, gpufft_stream_t stream);
+
+/* Replaces GPU_FFT(T* device_fix_inout, COMPLEX<T>* device_Complex64_inout,
+ * COMPLEX<T>* root_of_unity_table, fft_configuration<T> cfg, int batch_size,
+ * bool multiplication) — reference fft.cuh:126-132, fft.cu:600-725.
+ * Forward: reals in real_inout -> complex spectra in temp. Inverse: spectra in
+ * temp (product of the two halves when multiplication) -> real parts in
+ * real_inout. With zero_padding the upper half of every forward input vector
+ * is taken as zero and not read. */
+int gpufft_fft_r2r_f32(float* real_inout, void* temp, const void* root_table, int n_power,
+                       int fft_type, int reduction_poly, int zero_padding, float mod_inverse_re,
+                       float mod_inverse_im, int batch, int multiplication, gpufft_stream_t stream);
+int gpufft_fft_r2r_f64(double* real_inout, void* temp, const void* root_table, int n_power,
+                       int fft_type, int reduction_poly, int zero_padding, double mod_inverse_re,
+                       double mod_inverse_im, int batch, int multiplication, gpufft_stream_t stream);
+
+/* Replaces GPU_FFNT(T* device_inout, COMPLEX<T>* device_temp,
+ * COMPLEX<T>* twist_table, COMPLEX<T>* root_of_unity_table,
+ * fft_configuration<T> cfg, int batch_size, bool multiplication)
+ * — reference fft.cuh:269-273, fft.cu:1386-1515.
+ * N = 2^n_power reals per polynomial, transforms of N/2 complex. Forward: fold,
+ * twist, transform into temp. Inverse (twist_table = the UNTWIST table, as
+ * the reference's callers pass it): product, inverse transform, scale by
+ * mod_inverse, untwist, unfold into inout. */
+int gpufft_ffnt_f32(float* inout, void* temp, const void* twist_table, const void* root_table,
+                    int n_power, int fft_type, float mod_inverse_re, float mod_inverse_im, int batch,
+                    int multiplication, gpufft_stream_t stream);
+int gpufft_ffnt_f64(double* inout, void* temp, const void* twist_table, const void* root_table,
+                    int n_power, int fft_type, double mod_inverse_re, double mod_inverse_im, int batch,
+                    int multiplication, gpufft_stream_t stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* GPUFFT_B200_H */
