@@ -69,6 +69,15 @@ def lib() -> ctypes.CDLL:
         L.gpufft_fft_r2r_f64.argtypes = [vp, vp, vp, i, i, i, i, d, d, i, i, vp]
         L.gpufft_ffnt_f32.argtypes = [vp, vp, vp, vp, i, i, f, f, i, i, vp]
         L.gpufft_ffnt_f64.argtypes = [vp, vp, vp, vp, i, i, d, d, i, i, vp]
+        sz = ctypes.c_size_t
+        L.gpufft_ffnt_tables_count.argtypes = [i]
+        L.gpufft_ffnt_tables_count.restype = sz
+        L.gpufft_ffnt_make_tables_f32.argtypes = [i, vp, vp]
+        L.gpufft_ffnt_make_tables_f64.argtypes = [i, vp, vp]
+        L.gpufft_negacyclic_mul_workspace_bytes.argtypes = [i, i, i]
+        L.gpufft_negacyclic_mul_workspace_bytes.restype = sz
+        L.gpufft_negacyclic_mul_f32.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
+        L.gpufft_negacyclic_mul_f64.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
         L.gpufft_last_cuda_error.restype = i
         L.gpufft_status_string.restype = ctypes.c_char_p
         L.gpufft_status_string.argtypes = [i]
@@ -161,3 +170,52 @@ def GPU_FFNT(inout, temp, twist_table, root_table, cfg, batch, multiplication):
            complex(cfg.mod_inverse).real, complex(cfg.mod_inverse).imag, int(batch), int(bool(multiplication)),
            _stream_handle(cfg.stream))
     check(st, "GPU_FFNT")
+
+
+# ---------------------------------------------------------------------------
+# Native fused products (one call per batch of products; no reference
+# counterpart as a single call, see include/gpufft_b200.h)
+# ---------------------------------------------------------------------------
+def ffnt_tables(n_power: int, dtype="f64", device=None, stream=None):
+    """Device twiddle block [roots | inverse roots | twist | untwist] for N = 2^n_power,
+    generated on the GPU with sincospi."""
+    import torch
+    L = lib()
+    cnt = L.gpufft_ffnt_tables_count(n_power)
+    if cnt == 0:
+        raise ValueError("Invalid n_power range!")
+    f64 = dtype in ("f64", torch.float64, torch.complex128)
+    t = torch.empty(cnt, dtype=torch.complex128 if f64 else torch.complex64, device=device or "cuda")
+    f = L.gpufft_ffnt_make_tables_f64 if f64 else L.gpufft_ffnt_make_tables_f32
+    check(f(n_power, t.data_ptr(), _stream_handle(stream)), "ffnt_tables")
+    return t
+
+
+def negacyclic_mul_workspace_bytes(n_power: int, batch: int, precision_bits: int) -> int:
+    return int(lib().gpufft_negacyclic_mul_workspace_bytes(n_power, batch, precision_bits))
+
+
+def negacyclic_mul(a, b, out=None, tables=None, workspace=None, stream=None):
+    """c = a * b mod (X^N + 1) for every row of the (batch, N) float tensors a, b.
+    Not rounded, as GPU_FFNT."""
+    import torch
+    batch, n = a.shape
+    n_power = n.bit_length() - 1
+    if (1 << n_power) != n or b.shape != a.shape or a.dtype != b.dtype:
+        raise GpufftError(ERROR_INVALID_VALUE, "a and b must be (batch, 2^k) tensors of one dtype")
+    f64 = a.dtype == torch.float64
+    bits = 64 if f64 else 32
+    if tables is None:
+        tables = ffnt_tables(n_power, "f64" if f64 else "f32", a.device, stream)
+    if out is None:
+        out = torch.empty_like(a)
+    need = negacyclic_mul_workspace_bytes(n_power, batch, bits)
+    if workspace is None and need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=a.device)
+    ws_ptr = workspace.data_ptr() if workspace is not None else None
+    ws_len = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    L = lib()
+    f = L.gpufft_negacyclic_mul_f64 if f64 else L.gpufft_negacyclic_mul_f32
+    check(f(_ptr(a), _ptr(b), _ptr(out), n_power, batch, _ptr(tables), ws_ptr, ws_len, _stream_handle(stream)),
+          "negacyclic_mul")
+    return out

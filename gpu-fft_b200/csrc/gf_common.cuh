@@ -72,9 +72,9 @@ int set_cuda_error(cudaError_t e);
 int check_launch();
 
 // Opt a kernel into more than 48 KB of dynamic shared memory, once per device.
-template <typename K> int ensure_smem(K* kernel, size_t bytes)
+// `done` must be a per-kernel array of 64 ints (one slot per device ordinal).
+template <typename K> int ensure_smem(K* kernel, size_t bytes, int* done)
 {
-    static int done[64] = {0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_cuda_error(e);

@@ -182,4 +182,108 @@ __device__ __forceinline__ int run_pass_rounds(cx<T> (&x)[RPT], cx<T>* sm, const
     return wcur;
 }
 
+// ---------------------------------------------------------------------------
+// Two arrays through the same rounds (the two operands of a product share the
+// element placement, the twiddles and the index arithmetic).
+// ---------------------------------------------------------------------------
+template <typename T, bool FWD, int A, int RB>
+__device__ __forceinline__ void round_net2(cx<T> (&x)[RPT], cx<T> (&y)[RPT], const cx<T>* __restrict__ tw,
+                                           const TwCtx& c, int ebase, int wlo)
+{
+#pragma unroll
+    for (int k = 0; k < RB; k++)
+    {
+        const int pb = FWD ? (A + RB - 1 - k) : (A + k);
+        const int nhi = A + RB - 1 - pb;
+        const int p = wlo + pb;
+        const int u = c.qoff + c.L - 1 - p;
+        const long long gbase = (c.g << u) + (c.neg ? (1LL << (c.s0 + u)) : 0LL);
+#pragma unroll
+        for (int h = 0; h < (1 << nhi); h++)
+        {
+            const int rrep = h << (pb + 1);
+            const int e = ebase | (rrep << wlo);
+            const int q = (e >> c.qoff) & c.qmask;
+            const cx<T> w = ldg<T>(tw + gbase + (q >> (c.L - u)));
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+            {
+                if (r & (1 << pb)) continue;
+                if (((r >> (pb + 1)) & ((1 << nhi) - 1)) != h) continue;
+                if (FWD)
+                {
+                    ct_bfly<T>(x[r], x[r | (1 << pb)], w);
+                    ct_bfly<T>(y[r], y[r | (1 << pb)], w);
+                }
+                else
+                {
+                    gs_bfly<T>(x[r], x[r | (1 << pb)], w);
+                    gs_bfly<T>(y[r], y[r | (1 << pb)], w);
+                }
+            }
+        }
+    }
+}
+
+template <typename T, bool FWD>
+__device__ __forceinline__ void run_round2(cx<T> (&x)[RPT], cx<T> (&y)[RPT], const cx<T>* __restrict__ tw,
+                                           const TwCtx& c, int ebase, int wlo, int a, int rb)
+{
+    switch ((a << 3) | rb)
+    {
+    case (0 << 3) | 1: round_net2<T, FWD, 0, 1>(x, y, tw, c, ebase, wlo); break;
+    case (0 << 3) | 2: round_net2<T, FWD, 0, 2>(x, y, tw, c, ebase, wlo); break;
+    case (0 << 3) | 3: round_net2<T, FWD, 0, 3>(x, y, tw, c, ebase, wlo); break;
+    case (0 << 3) | 4: round_net2<T, FWD, 0, 4>(x, y, tw, c, ebase, wlo); break;
+    case (1 << 3) | 1: round_net2<T, FWD, 1, 1>(x, y, tw, c, ebase, wlo); break;
+    case (1 << 3) | 2: round_net2<T, FWD, 1, 2>(x, y, tw, c, ebase, wlo); break;
+    case (1 << 3) | 3: round_net2<T, FWD, 1, 3>(x, y, tw, c, ebase, wlo); break;
+    case (2 << 3) | 1: round_net2<T, FWD, 2, 1>(x, y, tw, c, ebase, wlo); break;
+    case (2 << 3) | 2: round_net2<T, FWD, 2, 2>(x, y, tw, c, ebase, wlo); break;
+    case (3 << 3) | 1: round_net2<T, FWD, 3, 1>(x, y, tw, c, ebase, wlo); break;
+    default: break;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void transpose2(cx<T> (&x)[RPT], cx<T> (&y)[RPT], cx<T>* sx, cx<T>* sy, int t, int wa,
+                                           int wb)
+{
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+    {
+        const int s = spad(e_of(t, wa, r));
+        sx[s] = x[r];
+        sy[s] = y[r];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+    {
+        const int s = spad(e_of(t, wb, r));
+        x[r] = sx[s];
+        y[r] = sy[s];
+    }
+}
+
+template <typename T, bool FWD>
+__device__ __forceinline__ int run_pass_rounds2(cx<T> (&x)[RPT], cx<T> (&y)[RPT], cx<T>* sx, cx<T>* sy,
+                                                const cx<T>* __restrict__ tw, const TwCtx& c, const Rounds& R,
+                                                int t)
+{
+    int wcur = R.lo[0] & ~3;
+    for (int i = 0; i < R.n; i++)
+    {
+        const int wlo = R.lo[i] & ~3;
+        if (wlo != wcur)
+        {
+            transpose2<T>(x, y, sx, sy, t, wcur, wlo);
+            wcur = wlo;
+        }
+        run_round2<T, FWD>(x, y, tw, c, e_of(t, wlo, 0), wlo, R.lo[i] - wlo, R.hi[i] - R.lo[i]);
+    }
+    return wcur;
+}
+
 } // namespace gfb

@@ -1,0 +1,311 @@
+// gpufft-b200: native fused negacyclic product c = a * b mod (X^N + 1).
+//
+// The product is the reference's FFNT chain (fold f_j + i f_{j+N/2}, twist by
+// e^{i pi j / N}, half-length FFT, pointwise product, inverse, scale, untwist,
+// unfold: reference fft.cu:1013-1384, fft_cpu.cu:301-432) fused so that the
+// two spectra are never written out as a caller-visible intermediate:
+//
+//   N <= 8192:  one kernel. A CTA loads both operands of 4096/(N/2) products,
+//               runs every forward stage on both in registers (shared twiddles
+//               and index arithmetic), multiplies, runs every inverse stage,
+//               untwists and writes the real product: one HBM read of a and b
+//               and one HBM write of c.
+//   N > 8192:   three kernels per wave of products -- the first forward pass
+//               (strided, fold+twist fused into the load), the fused last pass
+//               (forward both, multiply, inverse, in registers) and the last
+//               inverse pass (strided, scale+untwist+unfold fused into the
+//               store). The two spectra of a wave live in a caller-provided
+//               workspace sized to stay resident in the 126 MB L2.
+//
+// Twiddles come from gpufft_ffnt_make_tables_*, generated on the device with
+// sincospi in double precision (then rounded to float for the f32 path).
+#include "gf_pass.cuh"
+
+namespace gfb
+{
+
+// ---------------------------------------------------------------------------
+// device twiddle tables:  [roots M/2 | inverse roots M/2 | twist M | untwist M]
+// roots[i] = e^{+2 pi i bitrev_{m-1}(i) / M}, twist[j] = e^{+i pi j / N}, M = N/2
+// (the values of the reference's ReverseRootTable_ffnt / twist_table_ffnt,
+// fft_cpu.cu:251-297, 435-473, computed here in double precision).
+// ---------------------------------------------------------------------------
+template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
+{
+    const long long M = 1LL << m;
+    const long long H = M >> 1;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < H)
+    {
+        const unsigned br = (m > 1) ? (__brev((unsigned)i) >> (33 - m)) : 0u;
+        double s, c;
+        sincospi(2.0 * (double)br / (double)M, &s, &c);
+        tab[i] = mk<T>((T)c, (T)s);
+        tab[H + i] = mk<T>((T)c, (T)-s);
+    }
+    if (i < M)
+    {
+        double s, c;
+        sincospi((double)i / (double)(2 * M), &s, &c);
+        tab[2 * H + i] = mk<T>((T)c, (T)s);
+        tab[2 * H + M + i] = mk<T>((T)c, (T)-s);
+    }
+}
+
+template <typename T> struct FusedArgs
+{
+    const T* a;
+    const T* b;
+    T* c;
+    cx<T>* ws;
+    const cx<T>* roots;
+    const cx<T>* inv_roots;
+    const cx<T>* twist;
+    const cx<T>* untwist;
+    T scale;
+    long long batch; // products handled by this launch
+    PassGeo geo;
+};
+
+template <typename T, bool SINGLE>
+__global__ void __launch_bounds__(NTHR, 1) fused_kernel(const FusedArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* sx = reinterpret_cast<cx<T>*>(smraw);
+    cx<T>* sy = sx + SMEM_ELEMS;
+    const int t = threadIdx.x;
+    const long long cta = blockIdx.x;
+    const PassGeo& G = a.geo;
+    const long long M = 1LL << G.m;
+
+    TwCtx c;
+    c.qoff = 0;
+    c.L = G.L;
+    c.qmask = (1 << G.L) - 1;
+    c.s0 = G.s0;
+    c.neg = 0;
+    c.g = cta_group(G, cta);
+
+    const Rounds Rf = make_rounds(0, G.L, true);
+    const Rounds Ri = make_rounds(0, G.L, false);
+    const int w0 = Rf.lo[0] & ~3;
+
+    cx<T> x[RPT], y[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+    {
+        const Where w = locate(G, cta, e_of(t, w0, r));
+        if (w.b < a.batch)
+        {
+            if (SINGLE)
+            {
+                const cx<T> tw = ldg<T>(a.twist + w.j);
+                const T* pa = a.a + w.b * 2 * M + w.j;
+                const T* pb = a.b + w.b * 2 * M + w.j;
+                x[r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
+                y[r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
+            }
+            else
+            {
+                x[r] = a.ws[w.b * M + w.j];
+                y[r] = a.ws[(a.batch + w.b) * M + w.j];
+            }
+        }
+        else
+        {
+            x[r] = mk<T>(T(0), T(0));
+            y[r] = x[r];
+        }
+    }
+
+    run_pass_rounds2<T, true>(x, y, sx, sy, a.roots, c, Rf, t);
+#pragma unroll
+    for (int r = 0; r < RPT; r++) x[r] = cmul<T>(x[r], y[r]);
+    const int wl = run_pass_rounds<T, false>(x, sx, a.inv_roots, c, Ri, t);
+
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+    {
+        const Where w = locate(G, cta, e_of(t, wl, r));
+        if (w.b >= a.batch) continue;
+        if (SINGLE)
+        {
+            cx<T> v = cmul<T>(cmul<T>(x[r], mk<T>(a.scale, T(0))), ldg<T>(a.untwist + w.j));
+            T* pc = a.c + w.b * 2 * M + w.j;
+            st_stream(pc, v.x);
+            st_stream(pc + M, v.y);
+        }
+        else
+        {
+            a.ws[w.b * M + w.j] = x[r];
+        }
+    }
+}
+
+template <typename T, bool SINGLE> static int launch_fused(const FusedArgs<T>& a, long long ctas, cudaStream_t s)
+{
+    if (ctas <= 0) return GPUFFT_SUCCESS;
+    if (ctas > 0x7fffffffLL) return GPUFFT_ERROR_INVALID_VALUE;
+    const size_t smem = 2 * sizeof(cx<T>) * SMEM_ELEMS;
+    static int smem_done[64] = {0};
+    int st = ensure_smem(fused_kernel<T, SINGLE>, smem, smem_done);
+    if (st) return st;
+    fused_kernel<T, SINGLE><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
+    return check_launch();
+}
+
+constexpr int NATIVE_MIN_NPOWER = 2;
+constexpr int NATIVE_MAX_NPOWER = 22; // two-pass plans: M = N/2 <= 2^21
+constexpr size_t WAVE_TARGET_BYTES = 48ull << 20;
+
+static long long wave_products(int n_power, long long batch, size_t cx_bytes)
+{
+    const int m = n_power - 1;
+    if (m <= EBITS) return batch;
+    const size_t per = 2 * ((size_t)1 << m) * cx_bytes;
+    long long w = (long long)(WAVE_TARGET_BYTES / per);
+    if (w < 1) w = 1;
+    return w < batch ? w : batch;
+}
+
+template <typename T>
+static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, const void* tables, void* ws,
+                          size_t ws_bytes, cudaStream_t s)
+{
+    if (n_power < NATIVE_MIN_NPOWER || n_power > NATIVE_MAX_NPOWER) return GPUFFT_ERROR_INVALID_N_POWER;
+    if (!a || !b || !c || !tables || batch <= 0) return GPUFFT_ERROR_INVALID_VALUE;
+    if ((uintptr_t)a % sizeof(T) || (uintptr_t)b % sizeof(T) || (uintptr_t)c % sizeof(T) ||
+        (uintptr_t)tables % sizeof(cx<T>) || (uintptr_t)ws % sizeof(cx<T>))
+        return GPUFFT_ERROR_MISALIGNED;
+    const int m = n_power - 1;
+    const long long M = 1LL << m;
+    const auto* tab = reinterpret_cast<const cx<T>*>(tables);
+    FusedArgs<T> f{};
+    f.roots = tab;
+    f.inv_roots = tab + M / 2;
+    f.twist = tab + M;
+    f.untwist = tab + 2 * M;
+    f.scale = (T)(1.0 / (double)M);
+
+    if (m <= EBITS)
+    {
+        f.a = a;
+        f.b = b;
+        f.c = c;
+        f.batch = batch;
+        f.geo = PassGeo{};
+        f.geo.m = m;
+        f.geo.L = m;
+        f.geo.contig = 1;
+        const long long ctas = ((long long)batch * M + ECTA - 1) / ECTA;
+        return launch_fused<T, true>(f, ctas, s);
+    }
+
+    long long W = wave_products(n_power, batch, sizeof(cx<T>));
+    const size_t per = 2 * (size_t)M * sizeof(cx<T>);
+    if (!ws || ws_bytes < per) return GPUFFT_ERROR_WORKSPACE;
+    if ((size_t)W * per > ws_bytes) W = (long long)(ws_bytes / per);
+    cx<T>* wsp = reinterpret_cast<cx<T>*>(ws);
+    const Plan p = make_plan(m);
+    for (long long p0 = 0; p0 < batch; p0 += W)
+    {
+        const long long w = (batch - p0) < W ? (batch - p0) : W;
+        // 1. first forward pass of both operands: fold + twist in the load
+        {
+            long long ctas = 0;
+            PassArgs<T> k{};
+            k.geo = pass_geo(p, 0, m, 0, 2 * w, &ctas);
+            k.in = a + p0 * 2 * M;
+            k.in2 = b + p0 * 2 * M;
+            k.split = w;
+            k.out = wsp;
+            k.table = f.roots;
+            k.twist = f.twist;
+            k.batch = 2 * w;
+            int st = launch_pass<T, true, IN_FOLD2, OUT_CPX>(k, ctas, s);
+            if (st) return st;
+        }
+        // 2. last forward pass of both, product, first inverse pass
+        {
+            long long ctas = 0;
+            f.geo = pass_geo(p, 1, m, 0, w, &ctas);
+            f.ws = wsp;
+            f.batch = w;
+            int st = launch_fused<T, false>(f, ctas, s);
+            if (st) return st;
+        }
+        // 3. last inverse pass: scale, untwist, unfold into c
+        {
+            long long ctas = 0;
+            PassArgs<T> k{};
+            k.geo = pass_geo(p, 0, m, 0, w, &ctas);
+            k.in = wsp;
+            k.out = c + p0 * 2 * M;
+            k.table = f.inv_roots;
+            k.twist = f.untwist;
+            k.scale = mk<T>(f.scale, T(0));
+            k.do_scale = 1;
+            k.batch = w;
+            int st = launch_pass<T, false, IN_CPX, OUT_UNFOLD>(k, ctas, s);
+            if (st) return st;
+        }
+    }
+    return GPUFFT_SUCCESS;
+}
+
+template <typename T> static int make_tables(int n_power, void* tables, cudaStream_t s)
+{
+    if (n_power < NATIVE_MIN_NPOWER || n_power > 25) return GPUFFT_ERROR_INVALID_N_POWER;
+    if (!tables) return GPUFFT_ERROR_INVALID_VALUE;
+    if ((uintptr_t)tables % sizeof(cx<T>)) return GPUFFT_ERROR_MISALIGNED;
+    const int m = n_power - 1;
+    const long long M = 1LL << m;
+    const int thr = 256;
+    const long long blocks = (M + thr - 1) / thr;
+    ffnt_tables_kernel<T><<<(unsigned)blocks, thr, 0, s>>>(reinterpret_cast<cx<T>*>(tables), m);
+    return check_launch();
+}
+
+} // namespace gfb
+
+extern "C" size_t gpufft_ffnt_tables_count(int n_power)
+{
+    if (n_power < gfb::NATIVE_MIN_NPOWER || n_power > 25) return 0;
+    // [roots M/2 | inverse roots M/2 | twist M | untwist M], M = N/2
+    return (size_t)3 << (n_power - 1);
+}
+
+extern "C" int gpufft_ffnt_make_tables_f32(int n_power, void* tables, gpufft_stream_t stream)
+{
+    return gfb::make_tables<float>(n_power, tables, (cudaStream_t)stream);
+}
+extern "C" int gpufft_ffnt_make_tables_f64(int n_power, void* tables, gpufft_stream_t stream)
+{
+    return gfb::make_tables<double>(n_power, tables, (cudaStream_t)stream);
+}
+
+extern "C" size_t gpufft_negacyclic_mul_workspace_bytes(int n_power, int batch, int precision_bits)
+{
+    if (n_power < gfb::NATIVE_MIN_NPOWER || n_power > gfb::NATIVE_MAX_NPOWER || batch <= 0) return 0;
+    if (precision_bits != 32 && precision_bits != 64) return 0;
+    const size_t cxb = precision_bits == 64 ? 16 : 8;
+    const int m = n_power - 1;
+    if (m <= gfb::EBITS) return 0;
+    const long long w = gfb::wave_products(n_power, batch, cxb);
+    return (size_t)w * 2 * ((size_t)1 << m) * cxb;
+}
+
+extern "C" int gpufft_negacyclic_mul_f32(const float* a, const float* b, float* c, int n_power, int batch,
+                                         const void* tables, void* workspace, size_t workspace_bytes,
+                                         gpufft_stream_t stream)
+{
+    return gfb::negacyclic_mul<float>(a, b, c, n_power, batch, tables, workspace, workspace_bytes,
+                                      (cudaStream_t)stream);
+}
+extern "C" int gpufft_negacyclic_mul_f64(const double* a, const double* b, double* c, int n_power, int batch,
+                                         const void* tables, void* workspace, size_t workspace_bytes,
+                                         gpufft_stream_t stream)
+{
+    return gfb::negacyclic_mul<double>(a, b, c, n_power, batch, tables, workspace, workspace_bytes,
+                                       (cudaStream_t)stream);
+}

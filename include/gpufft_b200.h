@@ -108,6 +108,47 @@ int gpufft_ffnt_f64(double* inout, void* temp, const void* twist_table, const vo
                     int n_power, int fft_type, double mod_inverse_re, double mod_inverse_im, int batch,
                     int multiplication, gpufft_stream_t stream);
 
+/* Host-side twiddle tables of the drop-in API, written to HOST buffers:
+ * FFT<T>(n).ReverseRootTable / InverseReverseRootTable (n complex each) and
+ * n_inverse (one T) — reference fft_cpu.cu:93-128, 200-226; and
+ * FFNT<T>(n) ReverseRootTable_ffnt / InverseReverseRootTable_ffnt /
+ * twist_table_ffnt / untwist_table_ffnt (n/2 complex each) — reference
+ * fft_cpu.cu:234-300, 435-473. Same values bit for bit. n is a power of two. */
+int gpufft_host_fft_tables_f32(int n, void* roots, void* inv_roots, void* n_inverse);
+int gpufft_host_fft_tables_f64(int n, void* roots, void* inv_roots, void* n_inverse);
+int gpufft_host_ffnt_tables_f32(int n, void* roots, void* inv_roots, void* twist, void* untwist);
+int gpufft_host_ffnt_tables_f64(int n, void* roots, void* inv_roots, void* twist, void* untwist);
+
+/* ------------------------------------------------------------------------ */
+/* Native fused products (no reference counterpart as single calls: each one */
+/* replaces the pair GPU_FFNT(FORWARD, 2*batch) + GPU_FFNT(INVERSE, batch,  */
+/* multiplication) of reference fft.cu:1386-1515 / example                  */
+/* test_ffnt_gpu_R_R.cu:145-157, without writing the spectra to memory).    */
+/* ------------------------------------------------------------------------ */
+
+/* Number of complex entries of the native FFNT twiddle block for N = 2^n_power:
+ * [roots N/4 | inverse roots N/4 | twist N/2 | untwist N/2] (0 if out of range,
+ * n_power in [2, 25]). Same values as FFNT<T>::ReverseRootTable_ffnt,
+ * InverseReverseRootTable_ffnt, twist_table_ffnt, untwist_table_ffnt
+ * (reference fft_cpu.cu:435-473), computed on the device with sincospi. */
+size_t gpufft_ffnt_tables_count(int n_power);
+int gpufft_ffnt_make_tables_f32(int n_power, void* tables, gpufft_stream_t stream);
+int gpufft_ffnt_make_tables_f64(int n_power, void* tables, gpufft_stream_t stream);
+
+/* Workspace for gpufft_negacyclic_mul_* (precision_bits 32 or 64); 0 when the
+ * ring needs none (N <= 8192). Passing more lets larger waves run per launch. */
+size_t gpufft_negacyclic_mul_workspace_bytes(int n_power, int batch, int precision_bits);
+
+/* c[k] = a[k] * b[k] mod (X^N + 1) for k < batch, N = 2^n_power in [4, 2^22].
+ * a, b, c: batch x N reals (row-major); c may alias a or b. `tables` is the
+ * native twiddle block above. The output is not rounded (as GPU_FFNT). */
+int gpufft_negacyclic_mul_f32(const float* a, const float* b, float* c, int n_power, int batch,
+                              const void* tables, void* workspace, size_t workspace_bytes,
+                              gpufft_stream_t stream);
+int gpufft_negacyclic_mul_f64(const double* a, const double* b, double* c, int n_power, int batch,
+                              const void* tables, void* workspace, size_t workspace_bytes,
+                              gpufft_stream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

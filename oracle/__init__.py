@@ -80,7 +80,7 @@ def ref():
         R.ref_bitreverse.argtypes = [_c_int, _c_int]
         R.ref_schoolbook_negacyclic_u64.argtypes = [_u64p, _u64p, ctypes.c_uint64, _c_int, _u64p]
         R.ref_schoolbook_linear_i32.argtypes = [_i32p, _i32p, ctypes.c_int32, _c_int, _i32p]
-        R.ref_bench_ffnt_mult_f64.argtypes = [_c_int, _c_int, _c_int, _u64p, _u64p, _u64p]
+        R.ref_bench_ffnt_mult_f64.argtypes = [_c_int, _c_int, _c_int, _c_int, _u64p, _u64p, _u64p]
         R.ref_bench_ffnt_mult_f64.restype = ctypes.c_double
         R.ref_linear_product_f64.argtypes = [_c_int, _i64p, _i64p, _i64p]
         _REF = R

@@ -121,9 +121,10 @@ void ref_linear_product_f64(int n, const int64_t* a, const int64_t* b, int64_t* 
 // CPU baseline: FFNT<double>::MULT (fft_cpu.cu:301-432), one independent product
 // per host thread, each thread owning its FFNT object; the timed region covers
 // the MULT calls only (table construction excluded). Products are taken
-// round-robin from `a`/`b` (count of them, each n coefficients). Returns seconds.
-double ref_bench_ffnt_mult_f64(int n, int count, int threads, const uint64_t* a, const uint64_t* b,
-                               uint64_t* out)
+// round-robin from the `distinct` input pairs in `a`/`b` (n coefficients each;
+// `out` holds `distinct` results). Returns seconds.
+double ref_bench_ffnt_mult_f64(int n, int count, int distinct, int threads, const uint64_t* a,
+                               const uint64_t* b, uint64_t* out)
 {
     if (threads < 1) threads = 1;
     std::vector<FFNT<double>*> gens(threads);
@@ -137,10 +138,11 @@ double ref_bench_ffnt_mult_f64(int n, int count, int threads, const uint64_t* a,
             {
                 for (int p = t; p < count; p += threads)
                 {
-                    std::vector<unsigned long long> va(a + (size_t)p * n, a + (size_t)(p + 1) * n);
-                    std::vector<unsigned long long> vb(b + (size_t)p * n, b + (size_t)(p + 1) * n);
+                    const size_t q = (size_t)(p % distinct);
+                    std::vector<unsigned long long> va(a + q * n, a + (q + 1) * n);
+                    std::vector<unsigned long long> vb(b + q * n, b + (q + 1) * n);
                     auto r = gens[t]->MULT(va, vb);
-                    std::memcpy(out + (size_t)p * n, r.data(), sizeof(uint64_t) * n);
+                    std::memcpy(out + q * n, r.data(), sizeof(uint64_t) * n);
                 }
             });
     }

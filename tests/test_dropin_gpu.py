@@ -55,15 +55,16 @@ def test_c2c_forward_and_inverse_mult(gf, O, dev, T, n_power):
     x = (rng.standard_normal((2 * batch, M)) + 1j * rng.standard_normal((2 * batch, M))).astype(C)
     roots, _ = fft_table(O, n_power, T)
     inv_roots, _ = fft_table(O, n_power, T, inverse=True)
+    d_roots, d_inv = td(roots, dev), td(inv_roots, dev)
     buf = td(x.ravel(), dev)
     L = gf.lib()
     f = L.gpufft_fft_c2c_f64 if T == np.float64 else L.gpufft_fft_c2c_f32
-    gf.check(f(buf.data_ptr(), td(roots, dev).data_ptr(), n_power, 0, 1, 0, 1.0, 0.0, 2 * batch, 0, None), "fwd")
+    gf.check(f(buf.data_ptr(), d_roots.data_ptr(), n_power, 0, 1, 0, 1.0, 0.0, 2 * batch, 0, None), "fwd")
     want = O.gpu_fft_c2c(x.ravel(), roots, n_power, 0, 1, 1.0, 2 * batch, False)
     got = buf.cpu().numpy()
     assert rel_l2(got, want) < TOL[T]
     mi = 1.0 / M
-    gf.check(f(buf.data_ptr(), td(inv_roots, dev).data_ptr(), n_power, 1, 1, 0, mi, 0.0, batch, 1, None), "inv")
+    gf.check(f(buf.data_ptr(), d_inv.data_ptr(), n_power, 1, 1, 0, mi, 0.0, batch, 1, None), "inv")
     want2 = O.gpu_fft_c2c(want, inv_roots, n_power, 1, 1, mi, batch, True)
     got2 = buf.cpu().numpy()
     assert rel_l2(got2[: batch * M], want2[: batch * M]) < TOL[T]
@@ -83,11 +84,13 @@ def test_c2c_negacyclic_table_mode(gf, O, dev, T, n_power):
     buf = td(x.ravel(), dev)
     L = gf.lib()
     f = L.gpufft_fft_c2c_f64 if T == np.float64 else L.gpufft_fft_c2c_f32
-    gf.check(f(buf.data_ptr(), td(roots, dev).data_ptr(), n_power, 0, 0, 0, 1.0, 0.0, 2, 0, None), "fwd")
+    d_roots = td(roots, dev)
+    gf.check(f(buf.data_ptr(), d_roots.data_ptr(), n_power, 0, 0, 0, 1.0, 0.0, 2, 0, None), "fwd")
     want = O.gpu_fft_c2c(x.ravel(), roots, n_power, 0, 0, 1.0, 2, False)
     assert rel_l2(buf.cpu().numpy(), want) < TOL[T]
     inv_roots, _ = fft_table(O, n_power, T, neg=True, inverse=True)
-    gf.check(f(buf.data_ptr(), td(inv_roots, dev).data_ptr(), n_power, 1, 0, 0, 0.5, 0.25, 1, 1, None), "inv")
+    d_inv = td(inv_roots, dev)
+    gf.check(f(buf.data_ptr(), d_inv.data_ptr(), n_power, 1, 0, 0, 0.5, 0.25, 1, 1, None), "inv")
     want2 = O.gpu_fft_c2c(want, inv_roots, n_power, 1, 0, 0.5 + 0.25j, 1, True)
     assert rel_l2(buf.cpu().numpy()[:M], want2[:M]) < TOL[T]
 
@@ -108,16 +111,19 @@ def test_r2r_linear_product(gf, O, dev, T, n_power, zero_padding):
     temp = torch.zeros(2 * batch * M, dtype=torch.complex128 if T == np.float64 else torch.complex64, device=dev)
     L = gf.lib()
     f = L.gpufft_fft_r2r_f64 if T == np.float64 else L.gpufft_fft_r2r_f32
-    gf.check(f(rbuf.data_ptr(), temp.data_ptr(), td(roots, dev).data_ptr(), n_power, 0, 1, int(zero_padding),
+    d_roots, d_inv = td(roots, dev), td(inv_roots, dev)
+    gf.check(f(rbuf.data_ptr(), temp.data_ptr(), d_roots.data_ptr(), n_power, 0, 1, int(zero_padding),
                1.0, 0.0, 2 * batch, 0, None), "fwd")
     r1, t1 = O.gpu_fft_r2r(real.ravel(), np.zeros(2 * batch * M, cdt(T)), roots, n_power, 0, 1, 1.0, 2 * batch,
                            False)
     assert rel_l2(temp.cpu().numpy(), t1) < TOL[T]
-    gf.check(f(rbuf.data_ptr(), temp.data_ptr(), td(inv_roots, dev).data_ptr(), n_power, 1, 1, 0, float(ninv),
+    gf.check(f(rbuf.data_ptr(), temp.data_ptr(), d_inv.data_ptr(), n_power, 1, 1, 0, float(ninv),
                0.0, batch, 1, None), "inv")
     r2, _ = O.gpu_fft_r2r(r1, t1, inv_roots, n_power, 1, 1, float(ninv), batch, True)
     got = rbuf.cpu().numpy()
     assert rel_l2(got[: batch * M], r2[: batch * M]) < TOL[T]
+    if T == np.float32 and n_power > 13:
+        return  # |c| reaches 2^29: beyond float's exact integers
     for k in range(batch):
         exact = O.wrap64(O.schoolbook(real[k, :n].astype(np.int64), real[batch + k, :n].astype(np.int64),
                                       O.LINEAR))
@@ -158,20 +164,22 @@ def test_ffnt_product(gf, O, dev, T, n_power):
     roots, inv_roots, twist, untwist = O.ffnt_tables(n, sfx)
     buf = td(ab.ravel(), dev)
     temp = torch.zeros(2 * batch * h, dtype=torch.complex128 if T == np.float64 else torch.complex64, device=dev)
+    # keep every device table alive for the duration of the calls
+    d_roots, d_inv, d_tw, d_utw = (td(x, dev) for x in (roots, inv_roots, twist, untwist))
     L = gf.lib()
     f = L.gpufft_ffnt_f64 if T == np.float64 else L.gpufft_ffnt_f32
-    gf.check(f(buf.data_ptr(), temp.data_ptr(), td(twist, dev).data_ptr(), td(roots, dev).data_ptr(), n_power, 0,
+    gf.check(f(buf.data_ptr(), temp.data_ptr(), d_tw.data_ptr(), d_roots.data_ptr(), n_power, 0,
                1.0, 0.0, 2 * batch, 0, None), "fwd")
     r1, t1 = O.gpu_ffnt(ab.ravel(), np.zeros(2 * batch * h, cdt(T)), twist, roots, n_power, 0, 1.0, 2 * batch,
                         False)
     assert rel_l2(temp.cpu().numpy(), t1) < TOL[T]
     mi = 1.0 / h
-    gf.check(f(buf.data_ptr(), temp.data_ptr(), td(untwist, dev).data_ptr(), td(inv_roots, dev).data_ptr(),
+    gf.check(f(buf.data_ptr(), temp.data_ptr(), d_utw.data_ptr(), d_inv.data_ptr(),
                n_power, 1, mi, 0.0, batch, 1, None), "inv")
     r2, _ = O.gpu_ffnt(r1, t1, untwist, inv_roots, n_power, 1, mi, batch, True)
     got = buf.cpu().numpy()
     assert rel_l2(got[: batch * n], r2[: batch * n]) < TOL[T]
-    if n_power <= 16:
+    if n_power <= (16 if T == np.float64 else 10):
         for k in range(batch):
             exact = O.wrap64(O.schoolbook(ab[k].astype(np.int64), ab[batch + k].astype(np.int64)))
             assert np.array_equal(np.rint(got[k * n:(k + 1) * n]).astype(np.int64), exact)
