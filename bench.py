@@ -39,7 +39,9 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--path", choices=["f64", "f32", "dropin_f64"], default="f64")
+    p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64"], default="split")
+    p.add_argument("--no-compare", dest="compare", action="store_false",
+                   help="time only --path (by default FP64 is timed beside it)")
     p.add_argument("--n-power", type=int, default=16)
     p.add_argument("--batch", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -69,7 +71,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -79,7 +81,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *exc):
         if self.proc:
@@ -89,10 +91,18 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, t_lo=None, t_hi=None):
+        """Median SM clock and active throttle reasons of the samples taken in
+        [t_lo, t_hi] (widened by 0.25 s each side when none falls inside)."""
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines
+        if t_lo is not None:
+            inside = [x for x in lines if t_lo <= x[0] <= t_hi]
+            if not inside:
+                inside = [x for x in lines if t_lo - 0.25 <= x[0] <= t_hi + 0.25]
+            lines = inside
+        for _, ln in lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -170,96 +180,69 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def main():
-    args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        return run_reference(args, rank, world)
-
-    import torch
-    import __graft_entry__
-    gf = __graft_entry__.load_package()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=dev)
-
-    n_power, batch = args.n_power, args.batch
+def make_path(gf, name, n_power, batch, dev, torch):
+    """(step(a, b, c), algorithmic bytes per product, input/output element types,
+    kernel launches per step) for one product path."""
     n = 1 << n_power
-    f64 = args.path in ("f64", "dropin_f64")
-    fdt = torch.float64 if f64 else torch.float32
-    esz = 8 if f64 else 4
-    a64, b64 = make_inputs(batch, n, rank)
-    a_host = a64.to(fdt).pin_memory()
-    b_host = b64.to(fdt).pin_memory()
-    c_host = torch.empty_like(a_host).pin_memory()
-    a = a_host.to(dev)
-    b = b_host.to(dev)
-    c = torch.empty_like(a)
-    stream = torch.cuda.current_stream()
-
-    if args.path in ("f64", "f32"):
+    m = n_power - 1
+    if name in ("f64", "f32"):
+        f64 = name == "f64"
         tables = gf.ffnt_tables(n_power, "f64" if f64 else "f32", dev)
         ws_bytes = gf.negacyclic_mul_workspace_bytes(n_power, batch, 64 if f64 else 32)
         ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
-        m = n_power - 1
-        waves = 1 if m <= 12 else -(-batch // max(1, ws_bytes // (2 * (1 << m) * 2 * esz)))
-        launches_per_step = 1 if m <= 12 else 3 * waves
+        esz = 8 if f64 else 4
+        per = 2 * (1 << m) * (16 if f64 else 8)
+        waves = 1 if m <= 12 else -(-batch // max(1, ws_bytes // per))
 
         def step(x, y, out):
             gf.negacyclic_mul(x, y, out=out, tables=tables, workspace=ws)
-        alg_bytes = 3 * n * esz * batch
-    else:
-        import numpy as np
-        import oracle as O  # table values only (host-side generators of the drop-in API)
-        roots, inv_roots, twist, untwist = [torch.from_numpy(np.ascontiguousarray(t)).to(dev)
-                                            for t in O.ffnt_tables(n, "f64")]
-        inout = torch.empty(2 * batch * n, dtype=torch.float64, device=dev)
-        temp = torch.empty(batch * n, dtype=torch.complex128, device=dev)
-        cf = gf.fft_configuration(n_power=n_power, fft_type=gf.FORWARD)
-        ci = gf.fft_configuration(n_power=n_power, fft_type=gf.INVERSE, mod_inverse=1.0 / (n // 2))
-        launches_per_step = 4 if n_power - 1 > 12 else 2
+        dt = torch.float64 if f64 else torch.float32
+        return step, 3 * n * esz, dt, dt, (1 if m <= 12 else 3 * waves)
+    if name == "split":
+        w, k = gf.split_plan(n_power, 24, True)
+        tables = gf.ffnt_tables(n_power, "f32", dev)
+        need = int(gf.lib().gpufft_negacyclic_mul_split_workspace_bytes(n_power, batch, k))
+        ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+        per = (4 * k - 1) * (1 << m) * 8
+        waves = -(-batch // max(1, need // per))
 
         def step(x, y, out):
-            inout[: batch * n].copy_(x.view(-1))
-            inout[batch * n:].copy_(y.view(-1))
-            gf.GPU_FFNT(inout, temp, twist, roots, cf, 2 * batch, False)
-            gf.GPU_FFNT(inout, temp, untwist, inv_roots, ci, batch, True)
-            out.view(-1).copy_(inout[: batch * n])
-        alg_bytes = 3 * n * 8 * batch
+            gf.negacyclic_mul_split(x, y, out=out, input_bits=24, non_negative=True, limbs=(w, k), tables=tables,
+                                    workspace=ws)
+        return step, 16 * n, torch.int32, torch.int64, (1 if m <= 12 else 3) * waves
+    # drop-in: the reference API's two GPU_FFNT calls (forward of 2*batch, inverse with product)
+    import numpy as np
+    roots, inv_roots, twist, untwist = [torch.from_numpy(np.ascontiguousarray(t)).to(dev)
+                                        for t in gf.host_ffnt_tables(n, "f64")]
+    inout = torch.empty(2 * batch * n, dtype=torch.float64, device=dev)
+    temp = torch.empty(batch * n, dtype=torch.complex128, device=dev)
+    cf = gf.fft_configuration(n_power=n_power, fft_type=gf.FORWARD)
+    ci = gf.fft_configuration(n_power=n_power, fft_type=gf.INVERSE, mod_inverse=1.0 / (n // 2))
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+    def step(x, y, out):
+        inout[: batch * n].copy_(x.view(-1))
+        inout[batch * n:].copy_(y.view(-1))
+        gf.GPU_FFNT(inout, temp, twist, roots, cf, 2 * batch, False)
+        gf.GPU_FFNT(inout, temp, untwist, inv_roots, ci, batch, True)
+        out.view(-1).copy_(inout[: batch * n])
+    return step, 3 * n * 8, torch.float64, torch.float64, (4 if m > 12 else 2)
 
-    def max_over_ranks(ms):
-        if dist is None:
-            return ms
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
-    # ---- device-resident timing
+def time_path(step, a, b, c, hosts, args, stream, torch, barrier, max_over_ranks):
+    """Device-resident and end-to-end timing of one path: returns (ms, ms_e2e, t0, t1)."""
+    a_host, b_host, c_host = hosts
     for _ in range(args.warmup):
         step(a, b, c)
     barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            step(a, b, c)
-        e1.record(stream)
-        barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(a, b, c)
+    e1.record(stream)
+    barrier()
+    t1 = time.time()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-
-    # ---- end to end through the public API with host buffers
     for _ in range(max(1, args.warmup // 2)):
         a.copy_(a_host, non_blocking=True)
         b.copy_(b_host, non_blocking=True)
@@ -276,29 +259,112 @@ def main():
     e3.record(stream)
     barrier()
     ms_e2e = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+    return ms, ms_e2e, t0, t1
 
-    # ---- correctness spot check on this rank's last product (exact when f64 holds it)
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import __graft_entry__
+    gf = __graft_entry__.load_package()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=120))
+
+    n_power, batch = args.n_power, args.batch
+    n = 1 << n_power
+    a64, b64 = make_inputs(batch, n, rank)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(ms):
+        if dist is None:
+            return ms
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     peak, peak_kind = peaks()
-    value = world * batch / (ms * 1e-3)
-    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    results = {}
+    paths = [args.path] + ([p for p in ("f64",) if p != args.path] if args.compare else [])
+    with ClockSampler(local) as clk:
+        time.sleep(0.5)  # let the sampler start before the timed regions
+        for name in paths:
+            step, alg, din, dout, launches = make_path(gf, name, n_power, batch, dev, torch)
+            a_host = a64.to(din).pin_memory()
+            b_host = b64.to(din).pin_memory()
+            c_host = torch.empty((batch, n), dtype=dout).pin_memory()
+            a, b = a_host.to(dev), b_host.to(dev)
+            c = torch.empty((batch, n), dtype=dout, device=dev)
+            ms, ms_e2e, t0, t1 = time_path(step, a, b, c, (a_host, b_host, c_host), args, stream, torch, barrier,
+                                           max_over_ranks)
+            achieved = alg * batch / (ms * 1e-3) / 1e9
+            results[name] = dict(ms=ms, ms_e2e=ms_e2e, t0=t0, t1=t1, alg=alg, launches=launches,
+                                 value=world * batch / (ms * 1e-3), achieved=achieved,
+                                 h2d=2 * batch * n * a_host.element_size(), d2h=batch * n * c_host.element_size(),
+                                 dtype={torch.float64: "f64", torch.float32: "f32", torch.int32: "f32"}[din],
+                                 c=c[:2].cpu() if rank == 0 else None)
+            del a, b, c, a_host, b_host, c_host
+        time.sleep(0.3)
+
+    main_r = results[args.path]
+    t_lo, t_hi = main_r["t0"], main_r["t1"]
     line = {
-        "metric": f"negacyclic poly-mults/s at N=2^{n_power}", "value": value, "unit": "products/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if f64 else "f32", "data": "synthetic (seeded uniform integers in [0, 2^24))",
+        "metric": f"negacyclic poly-mults/s at N=2^{n_power}", "value": main_r["value"], "unit": "products/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": main_r["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": main_r["dtype"],
+        "data": "synthetic (seeded uniform integers in [0, 2^24))",
         "config": {"workload": f"FFNT negacyclic product N=2^{n_power}, batch {batch} per GPU, "
                                f"coefficients in [0, 2^24), path {args.path}",
                    "ring_log2": n_power, "batch_per_gpu": batch, "path": args.path,
                    "l2": "inputs larger than L2 (no flush)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_product": alg_bytes // batch,
+        "roofline": {"bound": "hbm", "achieved": main_r["achieved"], "peak": peak, "unit": "GB/s",
+                     "frac": main_r["achieved"] / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_product": main_r["alg"],
                      "timed": "whole product chain (all launches of one step), CUDA events"},
-        "e2e": {"value": world * batch / (ms_e2e * 1e-3), "unit": "products/s",
-                "h2d_bytes_per_step": 2 * batch * n * esz, "d2h_bytes_per_step": batch * n * esz},
-        "gpu_launches": launches_per_step * args.steps,
-        "clocks": clk.summary(),
+        "e2e": {"value": world * batch / (main_r["ms_e2e"] * 1e-3), "unit": "products/s",
+                "h2d_bytes_per_step": main_r["h2d"], "d2h_bytes_per_step": main_r["d2h"]},
+        "gpu_launches": main_r["launches"] * args.steps,
+        "clocks": clk.summary(t_lo, t_hi),
     }
+    for name, r in results.items():
+        if name == args.path:
+            continue
+        line[name] = {"value": r["value"], "unit": "products/s", "ms_per_step": r["ms"],
+                      "roofline_frac": r["achieved"] / peak, "achieved_gbs": r["achieved"],
+                      "e2e_value": world * batch / (r["ms_e2e"] * 1e-3)}
+    if rank == 0:
+        # exactness spot check of the first product: 64 sampled coefficients
+        import numpy as np
+        import oracle as O
+        rng = np.random.default_rng(1)
+        idx = np.sort(rng.choice(n, 64, replace=False)).astype(np.int32)
+        want = O.wrap64(O.negacyclic_coeffs(a64[0].numpy(), b64[0].numpy(), idx))
+        for name, r in results.items():
+            got = r["c"][0].numpy()[idx]
+            if got.dtype != np.int64:
+                err = float(np.max(np.abs(got.astype(np.float64) - want.astype(np.float64))))
+                exact = bool(np.array_equal(np.rint(got).astype(np.int64), want))
+            else:
+                err, exact = 0.0, bool(np.array_equal(got, want))
+            tgt = line if name == args.path else line[name]
+            tgt["exact_on_sample"] = exact
+            tgt["max_abs_error_on_sample"] = err
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cnt = cpu_sample_count(n, threads)

@@ -78,6 +78,15 @@ def lib() -> ctypes.CDLL:
         L.gpufft_negacyclic_mul_workspace_bytes.restype = sz
         L.gpufft_negacyclic_mul_f32.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
         L.gpufft_negacyclic_mul_f64.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
+        L.gpufft_host_fft_tables_f32.argtypes = [i, vp, vp, vp]
+        L.gpufft_host_fft_tables_f64.argtypes = [i, vp, vp, vp]
+        L.gpufft_host_ffnt_tables_f32.argtypes = [i, vp, vp, vp, vp]
+        L.gpufft_host_ffnt_tables_f64.argtypes = [i, vp, vp, vp, vp]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.gpufft_split_plan.argtypes = [i, i, i, ip, ip]
+        L.gpufft_negacyclic_mul_split_workspace_bytes.argtypes = [i, i, i]
+        L.gpufft_negacyclic_mul_split_workspace_bytes.restype = sz
+        L.gpufft_negacyclic_mul_split_f32.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, vp, sz, vp, vp]
         L.gpufft_last_cuda_error.restype = i
         L.gpufft_status_string.restype = ctypes.c_char_p
         L.gpufft_status_string.argtypes = [i]
@@ -172,6 +181,31 @@ def GPU_FFNT(inout, temp, twist_table, root_table, cfg, batch, multiplication):
     check(st, "GPU_FFNT")
 
 
+def host_fft_tables(n: int, dtype="f64"):
+    """FFT<T>(n) tables on the host: (ReverseRootTable, InverseReverseRootTable, n_inverse)
+    as numpy arrays (reference fft_cpu.cu:93-128, 200-226)."""
+    import numpy as np
+    f64 = dtype in ("f64", np.float64)
+    C = np.complex128 if f64 else np.complex64
+    r, ri = np.zeros(n, C), np.zeros(n, C)
+    ninv = np.zeros(1, np.float64 if f64 else np.float32)
+    f = lib().gpufft_host_fft_tables_f64 if f64 else lib().gpufft_host_fft_tables_f32
+    check(f(n, r.ctypes.data, ri.ctypes.data, ninv.ctypes.data), "host_fft_tables")
+    return r, ri, ninv[0]
+
+
+def host_ffnt_tables(n: int, dtype="f64"):
+    """FFNT<T>(n) tables on the host: (ReverseRootTable_ffnt, InverseReverseRootTable_ffnt,
+    twist_table_ffnt, untwist_table_ffnt), n/2 entries each (reference fft_cpu.cu:234-300, 435-473)."""
+    import numpy as np
+    f64 = dtype in ("f64", np.float64)
+    C = np.complex128 if f64 else np.complex64
+    out = [np.zeros(n // 2, C) for _ in range(4)]
+    f = lib().gpufft_host_ffnt_tables_f64 if f64 else lib().gpufft_host_ffnt_tables_f32
+    check(f(n, *[o.ctypes.data for o in out]), "host_ffnt_tables")
+    return tuple(out)
+
+
 # ---------------------------------------------------------------------------
 # Native fused products (one call per batch of products; no reference
 # counterpart as a single call, see include/gpufft_b200.h)
@@ -219,3 +253,42 @@ def negacyclic_mul(a, b, out=None, tables=None, workspace=None, stream=None):
     check(f(_ptr(a), _ptr(b), _ptr(out), n_power, batch, _ptr(tables), ws_ptr, ws_len, _stream_handle(stream)),
           "negacyclic_mul")
     return out
+
+
+def split_plan(n_power: int, input_bits: int, non_negative: bool = False):
+    """(limb_bits, num_limbs) the library uses for exact FP32 split products."""
+    w, k = ctypes.c_int(), ctypes.c_int()
+    check(lib().gpufft_split_plan(n_power, input_bits, int(non_negative), ctypes.byref(w), ctypes.byref(k)),
+          "split_plan")
+    return w.value, k.value
+
+
+def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, limbs=None, tables=None,
+                         workspace=None, stream=None, return_error=False):
+    """Exact c = a * b mod (X^N + 1) for (batch, N) int32 tensors, computed with FP32
+    transforms on limbs; returns an int64 tensor (and the max pre-rounding error)."""
+    import torch
+    batch, n = a.shape
+    n_power = n.bit_length() - 1
+    if (1 << n_power) != n or b.shape != a.shape or a.dtype != torch.int32 or b.dtype != torch.int32:
+        raise GpufftError(ERROR_INVALID_VALUE, "a and b must be (batch, 2^k) int32 tensors")
+    if input_bits is None or non_negative is None:
+        mx = int(torch.maximum(a.abs().max(), b.abs().max()).item())
+        mn = int(torch.minimum(a.min(), b.min()).item())
+        input_bits = max(1, mx.bit_length()) if input_bits is None else input_bits
+        non_negative = (mn >= 0) if non_negative is None else non_negative
+    w, k = limbs if limbs is not None else split_plan(n_power, input_bits, non_negative)
+    if tables is None:
+        tables = ffnt_tables(n_power, "f32", a.device, stream)
+    if out is None:
+        out = torch.empty((batch, n), dtype=torch.int64, device=a.device)
+    need = int(lib().gpufft_negacyclic_mul_split_workspace_bytes(n_power, batch, k))
+    if workspace is None:
+        workspace = torch.empty(max(need, 1), dtype=torch.uint8, device=a.device)
+    err = torch.zeros(1, dtype=torch.float32, device=a.device)
+    st = lib().gpufft_negacyclic_mul_split_f32(
+        _ptr(a), _ptr(b), _ptr(out), n_power, batch, int(input_bits), int(bool(non_negative)), w, k,
+        _ptr(tables), workspace.data_ptr(), workspace.numel() * workspace.element_size(), err.data_ptr(),
+        _stream_handle(stream))
+    check(st, "negacyclic_mul_split")
+    return (out, err) if return_error else out

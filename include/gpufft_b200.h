@@ -149,6 +149,27 @@ int gpufft_negacyclic_mul_f64(const double* a, const double* b, double* c, int n
                               const void* tables, void* workspace, size_t workspace_bytes,
                               gpufft_stream_t stream);
 
+/* ------------------------------------------------------------------------ */
+/* FP32 split-precision negacyclic product with exact int64 output (no      */
+/* reference counterpart: the reference's products are plain FP32/FP64).     */
+/* ------------------------------------------------------------------------ */
+
+/* The limb plan (width, count) the library picks for rings of 2^n_power with
+ * |coefficients| < 2^input_bits (non_negative: all coefficients >= 0). */
+int gpufft_split_plan(int n_power, int input_bits, int non_negative, int* limb_bits, int* num_limbs);
+/* Workspace for gpufft_negacyclic_mul_split_f32 with num_limbs limbs. */
+size_t gpufft_negacyclic_mul_split_workspace_bytes(int n_power, int batch, int num_limbs);
+/* c[k] = a[k] * b[k] mod (X^N + 1), exact in int64 (wrapping mod 2^64), from
+ * int32 coefficients with |x| < 2^input_bits, N = 2^n_power in [4, 2^22].
+ * Limbs: limb_bits/num_limbs, or 0/0 for the plan of gpufft_split_plan.
+ * `tables` is the f32 native twiddle block (gpufft_ffnt_make_tables_f32).
+ * max_error (device pointer, may be NULL) receives the largest distance of a
+ * limb-group value to its nearest integer; the result is exact when < 0.5. */
+int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch,
+                                    int input_bits, int non_negative, int limb_bits, int num_limbs,
+                                    const void* tables, void* workspace, size_t workspace_bytes,
+                                    float* max_error, gpufft_stream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

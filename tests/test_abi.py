@@ -58,3 +58,34 @@ def test_python_mirror_range_check_matches_reference(gf):
     cfg.n_power = 25
     with pytest.raises(ValueError, match="Invalid n_power range!"):
         gf.GPU_FFNT(None, None, None, None, cfg, 1, False)
+
+
+@pytest.mark.parametrize("sfx", ["f64", "f32"])
+def test_host_table_generators_match_reference_bitwise(gf, O, sfx):
+    # the drop-in API's FFT<T>/FFNT<T> table generators (host code in the
+    # library) give the reference's tables bit for bit (golden fixtures made by
+    # the reference's own build, and the oracle for other sizes)
+    import numpy as np
+    gold = os.path.join(ROOT, "tests", "golden")
+    g = np.load(os.path.join(gold, f"fft_tables_{sfx}.npz"))
+    r, ri, ninv = gf.host_fft_tables(int(g["n"]), sfx)
+    T = np.float64 if sfx == "f64" else np.float32
+    assert np.array_equal(r.view(T), g["rev_roots"]) and np.array_equal(ri.view(T), g["rev_inv_roots"])
+    assert ninv == g["n_inverse"][0]
+    g = np.load(os.path.join(gold, f"ffnt_tables_{sfx}.npz"))
+    for got, key in zip(gf.host_ffnt_tables(int(g["n"]), sfx), ["rev_roots", "rev_inv_roots", "twist", "untwist"]):
+        assert np.array_equal(got.view(T), g[key]), key
+    for n in (4, 64, 1 << 15):
+        for got, want in zip(gf.host_ffnt_tables(n, sfx), O.ffnt_tables(n, sfx)):
+            assert np.array_equal(got, want)
+        r, ri, ninv = gf.host_fft_tables(n, sfx)
+        wr, wri, wn = O.fft_tables(n, sfx)
+        assert np.array_equal(r, wr) and np.array_equal(ri, wri) and ninv == wn
+
+
+def test_split_plan_host_logic(gf):
+    # limb plans picked by the error model (host-only, no GPU)
+    assert gf.split_plan(16, 24, True) == (5, 5)
+    w, k = gf.split_plan(12, 24, True)
+    assert w * k >= 24 and k <= 4
+    assert gf.split_plan(16, 16, False)[0] * gf.split_plan(16, 16, False)[1] >= 16

@@ -1,0 +1,63 @@
+"""GPU tests of the FP32 split-precision product: bit-exact int64 results
+against the exact __int128 schoolbook product, and the reported maximum
+pre-rounding error stays below 0.5 (the exactness criterion)."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def exact_rows(O, a, b, idx=None):
+    out = []
+    for k in range(a.shape[0]):
+        if idx is None:
+            out.append(O.wrap64(O.schoolbook(a[k].astype(np.int64), b[k].astype(np.int64))))
+        else:
+            out.append(O.wrap64(O.negacyclic_coeffs(a[k], b[k], idx)))
+    return np.stack(out)
+
+
+@pytest.mark.parametrize("n_power,batch,lo,hi", [
+    (2, 7, 0, 1 << 24), (5, 5, -(1 << 15), 1 << 15), (10, 9, 0, 1 << 24), (12, 3, -(1 << 20), 1 << 20),
+    (13, 3, 0, 1 << 24), (14, 2, -(1 << 15), 1 << 15), (15, 2, 0, 1 << 24), (16, 2, 0, 1 << 24),
+    (17, 1, -(1 << 15), 1 << 15)])
+def test_split_exact(gf, O, dev, n_power, batch, lo, hi):
+    rng = np.random.default_rng(4000 + n_power)
+    n = 1 << n_power
+    a = rng.integers(lo, hi, (batch, n)).astype(np.int32)
+    b = rng.integers(lo, hi, (batch, n)).astype(np.int32)
+    c, err = gf.negacyclic_mul_split(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev), return_error=True)
+    got = c.cpu().numpy()
+    e = float(err.item())
+    assert e < 0.5, e
+    if n_power <= 14:
+        assert np.array_equal(got, exact_rows(O, a, b))
+    else:  # 512 random coefficients per product against the exact O(N) formula
+        idx = np.sort(rng.choice(n, 512, replace=False)).astype(np.int32)
+        assert np.array_equal(got[:, idx], exact_rows(O, a, b, idx))
+
+
+def test_split_config3_full_batch(gf, O, dev):
+    # config 3 at N = 2^16, batch 256, coefficients uniform in [0, 2^24): exact on
+    # sampled coefficients of sampled products; error report below 0.5
+    rng = np.random.default_rng(3)
+    n, batch = 1 << 16, 256
+    a = rng.integers(0, 1 << 24, (batch, n)).astype(np.int32)
+    b = rng.integers(0, 1 << 24, (batch, n)).astype(np.int32)
+    c, err = gf.negacyclic_mul_split(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev), input_bits=24,
+                                     non_negative=True, return_error=True)
+    assert float(err.item()) < 0.5
+    got = c.cpu().numpy()
+    idx = np.sort(rng.choice(n, 128, replace=False)).astype(np.int32)
+    for k in (0, 77, 255):
+        assert np.array_equal(got[k, idx], O.wrap64(O.negacyclic_coeffs(a[k], b[k], idx)))
+
+
+def test_split_reports_inexact_plan(gf, dev):
+    # an under-sized limb plan (one 24-bit limb) is flagged by the error report
+    rng = np.random.default_rng(9)
+    n = 1 << 14
+    a = torch.from_numpy(rng.integers(0, 1 << 24, (1, n)).astype(np.int32)).to(dev)
+    _, err = gf.negacyclic_mul_split(a, a, input_bits=24, non_negative=True, limbs=(24, 1), return_error=True)
+    assert float(err.item()) >= 0.5
