@@ -16,7 +16,6 @@
 namespace gfb
 {
 
-// Dispatch helpers so that every (IN, OUT) pair used below is instantiated once.
 template <typename T>
 static int run_forward(int m, int neg, long long batch, const void* in, int in_kind, void* out,
                        const cx<T>* table, const cx<T>* twist, int zero_pad, cudaStream_t s)
@@ -33,14 +32,9 @@ static int run_forward(int m, int neg, long long batch, const void* in, int in_k
         a.in = (k == 0) ? in : out;
         a.out = out;
         a.zero_pad = (k == 0) ? zero_pad : 0;
-        int st;
-        const int ik = (k == 0) ? in_kind : IN_CPX;
-        if (ik == IN_CPX)
-            st = launch_pass<T, true, IN_CPX, OUT_CPX>(a, ctas, s);
-        else if (ik == IN_REAL)
-            st = launch_pass<T, true, IN_REAL, OUT_CPX>(a, ctas, s);
-        else
-            st = launch_pass<T, true, IN_FOLD, OUT_CPX>(a, ctas, s);
+        a.in_kind = (k == 0) ? in_kind : IN_CPX;
+        a.out_kind = OUT_CPX;
+        const int st = launch_pass<T, true>(a, p, k, ctas, s);
         if (st) return st;
     }
     return GPUFFT_SUCCESS;
@@ -69,27 +63,9 @@ static int run_inverse(int m, int neg, long long batch, void* work, int mult, lo
         const bool first = (k == p.np - 1), last = (k == 0);
         a.out = last ? out : work;
         a.do_scale = last ? 1 : 0;
-        const int ik = (first && mult) ? IN_PROD : IN_CPX;
-        const int ok = last ? out_kind : OUT_CPX;
-        int st;
-        if (ik == IN_PROD)
-        {
-            if (ok == OUT_CPX)
-                st = launch_pass<T, false, IN_PROD, OUT_CPX>(a, ctas, s);
-            else if (ok == OUT_REAL)
-                st = launch_pass<T, false, IN_PROD, OUT_REAL>(a, ctas, s);
-            else
-                st = launch_pass<T, false, IN_PROD, OUT_UNFOLD>(a, ctas, s);
-        }
-        else
-        {
-            if (ok == OUT_CPX)
-                st = launch_pass<T, false, IN_CPX, OUT_CPX>(a, ctas, s);
-            else if (ok == OUT_REAL)
-                st = launch_pass<T, false, IN_CPX, OUT_REAL>(a, ctas, s);
-            else
-                st = launch_pass<T, false, IN_CPX, OUT_UNFOLD>(a, ctas, s);
-        }
+        a.in_kind = (first && mult) ? IN_PROD : IN_CPX;
+        a.out_kind = last ? out_kind : OUT_CPX;
+        const int st = launch_pass<T, false>(a, p, k, ctas, s);
         if (st) return st;
     }
     return GPUFFT_SUCCESS;

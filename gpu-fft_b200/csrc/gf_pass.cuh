@@ -13,14 +13,24 @@ enum InKind
     IN_CPX = 0,  // complex vector (transform position j)
     IN_REAL = 1, // real promoted to complex (fft.cu:303-305)
     IN_FOLD = 2, // FFNT fold f_j + i f_{j+M} then twist (fft.cu:1057-1069)
-    IN_PROD = 3,  // product of the two complex operands (fft.cu:194-205, 1252-1263)
-    IN_FOLD2 = 4  // IN_FOLD with batch entries [0, split) from `in`, the rest from `in2`
+    IN_PROD = 3, // product of the two complex operands (fft.cu:194-205, 1252-1263)
+    IN_FOLD2 = 4 // IN_FOLD with batch entries [0, split) from `in`, the rest from `in2`
 };
 enum OutKind
 {
     OUT_CPX = 0,   // complex vector, optionally scaled by mod_inverse (fft.cu:246-253)
     OUT_REAL = 1,  // real part of the scaled value (fft.cu:499-514)
     OUT_UNFOLD = 2 // scale, untwist, unfold re -> j, im -> j+M (fft.cu:1366-1383)
+};
+
+// Geometry of one pass (stages [s0, s0+L) of a 2^m transform); L and the
+// strided/contiguous choice are template parameters of the kernels.
+struct PassGeo
+{
+    int m;    // log2 transform length
+    int s0;   // first stage of the pass
+    int neg;  // negacyclic (X^N+1) twiddle indexing
+    int pad_;
 };
 
 template <typename T> struct PassArgs
@@ -33,79 +43,81 @@ template <typename T> struct PassArgs
     cx<T> scale;
     long long prod_off; // element offset of the second operand (IN_PROD)
     long long batch;
-    PassGeo geo;
     long long split; // IN_FOLD2: batch entries taken from `in`
-    int zero_pad;    // forward first pass: the upper half of each input is zero
-    int do_scale;    // last inverse pass: multiply by scale
+    PassGeo geo;
+    int in_kind, out_kind;
+    int zero_pad; // forward first pass: the upper half of each input is zero
+    int do_scale; // last inverse pass: multiply by scale
 };
 
-// Locate CTA-local element e: transform index j and batch entry b.
-struct Where
+// Where the 16 registers of thread t (window W) live: batch entry b[r] and
+// transform index j[r] of every register, for a CTA `cta` of a pass with L
+// stages, strided (columns of the pass share a CTA) or contiguous.
+template <int L, bool STRIDED, int W> struct Tile
 {
-    long long b;
-    long long j;
+    long long b[RPT];
+    long long j[RPT];
+    long long g; // stage-s0 group (uniform over the CTA)
+
+    __device__ __forceinline__ Tile(const PassGeo& G, long long cta, int t)
+    {
+        const int eb = e_base<W>(t);
+        const long long M = 1LL << G.m;
+        if constexpr (STRIDED)
+        {
+            constexpr int CL = EBITS - L; // log2 columns per CTA
+            const int lgcpb = G.m - G.s0 - EBITS; // log2 column blocks per group
+            const long long bb = cta >> (G.m - EBITS);
+            const long long rem = cta & ((1LL << (G.m - EBITS)) - 1);
+            g = rem >> lgcpb;
+            const long long cblk = rem & ((1LL << lgcpb) - 1);
+            const int sl = G.m - G.s0 - L; // log2 stride S
+            const long long j0 = (g << (G.m - G.s0)) + (cblk << CL) + (eb & ((1 << CL) - 1)) +
+                                 ((long long)(eb >> CL) << sl);
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+            {
+                // register bits r<<W split into column (below CL) and q (above) parts
+                const int e_r = r << W;
+                const int cpart = e_r & ((1 << CL) - 1);
+                const int qpart = e_r >> CL;
+                b[r] = bb;
+                j[r] = j0 + cpart + ((long long)qpart << sl);
+            }
+        }
+        else
+        {
+            const long long gi0 = cta * ECTA + eb;
+            g = ((cta * ECTA) >> L) & ((1LL << G.s0) - 1);
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+            {
+                const long long gi = gi0 + (r << W);
+                b[r] = gi >> G.m;
+                j[r] = gi & (M - 1);
+            }
+        }
+    }
 };
 
-__device__ __forceinline__ Where locate(const PassGeo& G, long long cta, int e)
-{
-    Where w;
-    const long long M = 1LL << G.m;
-    if (G.contig)
-    {
-        const long long gi = cta * ECTA + e;
-        w.b = gi >> G.m;
-        w.j = gi & (M - 1);
-    }
-    else
-    {
-        const long long S = 1LL << (G.m - G.s0 - G.L);
-        const int cols = 1 << G.cols_log;
-        const long long cpb = S >> G.cols_log;         // column blocks per group
-        const long long per_b = (1LL << G.s0) * cpb;   // CTAs per transform
-        w.b = cta / per_b;
-        const long long rem = cta - w.b * per_b;
-        const long long g = rem / cpb;
-        const long long cblk = rem - g * cpb;
-        const int c = e & (cols - 1);
-        const int q = e >> G.cols_log;
-        w.j = g * (M >> G.s0) + (long long)q * S + cblk * cols + c;
-    }
-    return w;
-}
-
-__device__ __forceinline__ long long cta_group(const PassGeo& G, long long cta)
-{
-    if (G.contig)
-    {
-        // sub-networks of 2^L elements; either s0 == 0 (g = 0) or one per CTA
-        const long long gi = cta * ECTA;
-        return (gi >> G.L) & ((1LL << G.s0) - 1);
-    }
-    const long long S = 1LL << (G.m - G.s0 - G.L);
-    const long long cpb = S >> G.cols_log;
-    const long long per_b = (1LL << G.s0) * cpb;
-    const long long rem = cta % per_b;
-    return rem / cpb;
-}
-
-template <typename T, int IN>
-__device__ __forceinline__ cx<T> load_elem(const PassArgs<T>& a, long long b, long long j)
+template <typename T>
+__device__ __forceinline__ cx<T> load_elem(const PassArgs<T>& a, int kind, long long b, long long j)
 {
     const long long M = 1LL << a.geo.m;
-    if (IN == IN_CPX)
+    if (kind == IN_CPX)
     {
         if (a.zero_pad && j >= (M >> 1)) return mk<T>(T(0), T(0));
         return reinterpret_cast<const cx<T>*>(a.in)[b * M + j];
     }
-    else if (IN == IN_REAL)
+    else if (kind == IN_REAL)
     {
         if (a.zero_pad && j >= (M >> 1)) return mk<T>(T(0), T(0));
         return mk<T>(reinterpret_cast<const T*>(a.in)[b * M + j], T(0));
     }
-    else if (IN == IN_FOLD || IN == IN_FOLD2)
+    else if (kind == IN_FOLD || kind == IN_FOLD2)
     {
         const T* base = reinterpret_cast<const T*>(a.in);
-        if (IN == IN_FOLD2 && b >= a.split)
+        if (kind == IN_FOLD2 && b >= a.split)
         {
             base = reinterpret_cast<const T*>(a.in2);
             b -= a.split;
@@ -121,16 +133,16 @@ __device__ __forceinline__ cx<T> load_elem(const PassArgs<T>& a, long long b, lo
     }
 }
 
-template <typename T, int OUT>
-__device__ __forceinline__ void store_elem(const PassArgs<T>& a, long long b, long long j, cx<T> v)
+template <typename T>
+__device__ __forceinline__ void store_elem(const PassArgs<T>& a, int kind, long long b, long long j, cx<T> v)
 {
     const long long M = 1LL << a.geo.m;
-    if (OUT == OUT_CPX)
+    if (kind == OUT_CPX)
     {
         if (a.do_scale) v = cmul<T>(v, a.scale);
         reinterpret_cast<cx<T>*>(a.out)[b * M + j] = v;
     }
-    else if (OUT == OUT_REAL)
+    else if (kind == OUT_REAL)
     {
         if (a.do_scale) v = cmul<T>(v, a.scale);
         reinterpret_cast<T*>(a.out)[b * M + j] = v.x;
@@ -144,41 +156,36 @@ __device__ __forceinline__ void store_elem(const PassArgs<T>& a, long long b, lo
     }
 }
 
-template <typename T, bool FWD, int IN, int OUT>
-__global__ void __launch_bounds__(NTHR) pass_kernel(const PassArgs<T> a)
+template <typename T, bool FWD, int L, bool STRIDED>
+__global__ void __launch_bounds__(NTHR, 2) pass_kernel(const PassArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+    constexpr int QOFF = STRIDED ? EBITS - L : 0;
+    using S = Sched<QOFF, L>;
+    constexpr int W0 = S::win(0, FWD), WL = S::win(S::n - 1, FWD);
     const int t = threadIdx.x;
     const long long cta = blockIdx.x;
-    const PassGeo& G = a.geo;
 
-    TwCtx c;
-    c.qoff = G.qoff;
-    c.L = G.L;
-    c.qmask = (1 << G.L) - 1;
-    c.s0 = G.s0;
-    c.neg = G.neg;
-    c.g = cta_group(G, cta);
-
-    const Rounds R = make_rounds(G.qoff, G.L, FWD);
-    const int w0 = R.lo[0] & ~3;
-
-    cx<T> x[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; r++)
+    cx<T> x[1][RPT];
     {
-        const Where w = locate(G, cta, e_of(t, w0, r));
-        x[r] = (w.b < a.batch) ? load_elem<T, IN>(a, w.b, w.j) : mk<T>(T(0), T(0));
+        const Tile<L, STRIDED, W0> tl(a.geo, cta, t);
+        const int kind = a.in_kind;
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            x[0][r] = (tl.b[r] < a.batch) ? load_elem<T>(a, kind, tl.b[r], tl.j[r]) : mk<T>(T(0), T(0));
     }
-
-    const int wl = run_pass_rounds<T, FWD>(x, sm, a.table, c, R, t);
-
-#pragma unroll
-    for (int r = 0; r < RPT; r++)
+    TwCtx c;
+    c.g = Tile<L, STRIDED, W0>(a.geo, cta, t).g;
+    c.s0 = a.geo.s0;
+    c.neg = a.geo.neg;
+    run_rounds<T, FWD, QOFF, L, 1>(x, sm, a.table, c, t);
     {
-        const Where w = locate(G, cta, e_of(t, wl, r));
-        if (w.b < a.batch) store_elem<T, OUT>(a, w.b, w.j, x[r]);
+        const Tile<L, STRIDED, WL> tl(a.geo, cta, t);
+        const int kind = a.out_kind;
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            if (tl.b[r] < a.batch) store_elem<T>(a, kind, tl.b[r], tl.j[r], x[0][r]);
     }
 }
 
@@ -191,6 +198,7 @@ struct Plan
     int L[3];
 };
 
+// m <= 12: one pass; 12 < m <= 21: (m-12, 12); 21 < m <= 24: (m-21, 9, 12)
 static inline Plan make_plan(int m)
 {
     Plan p;
@@ -215,45 +223,42 @@ static inline Plan make_plan(int m)
     return p;
 }
 
-// Geometry and grid size of pass k of plan p for a 2^m transform.
+// Geometry and grid size of pass k of plan p for `batch` transforms of 2^m.
 static inline PassGeo pass_geo(const Plan& p, int k, int m, int neg, long long batch, long long* ctas)
 {
     PassGeo G{};
     G.m = m;
-    G.L = p.L[k];
     G.s0 = 0;
     for (int i = 0; i < k; i++) G.s0 += p.L[i];
     G.neg = neg;
-    const long long M = 1LL << m;
     if (k == p.np - 1)
-    {
-        G.contig = 1;
-        G.qoff = 0;
-        G.cols_log = 0;
-        *ctas = (batch * M + ECTA - 1) / ECTA;
-    }
+        *ctas = ((batch << m) + ECTA - 1) / ECTA;
     else
-    {
-        G.contig = 0;
-        G.cols_log = EBITS - G.L;
-        G.qoff = G.cols_log;
-        const long long S = 1LL << (m - G.s0 - G.L);
-        *ctas = batch * (1LL << G.s0) * (S >> G.cols_log);
-    }
+        *ctas = batch << (m - EBITS);
     return G;
 }
 
-template <typename T, bool FWD, int IN, int OUT>
-static inline int launch_pass(PassArgs<T> a, long long ctas, cudaStream_t s)
+template <typename T, bool FWD, int L, bool STRIDED>
+static inline int launch_pass_shape(const PassArgs<T>& a, long long ctas, cudaStream_t s)
+{
+    const size_t smem = sizeof(cx<T>) * SMEM_ELEMS;
+    static int smem_done[64] = {0};
+    int st = ensure_smem(pass_kernel<T, FWD, L, STRIDED>, smem, smem_done);
+    if (st) return st;
+    pass_kernel<T, FWD, L, STRIDED><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
+    return check_launch();
+}
+
+// Launch pass k of plan p (the pass's L selects the compiled shape).
+template <typename T, bool FWD>
+static inline int launch_pass(const PassArgs<T>& a, const Plan& p, int k, long long ctas, cudaStream_t s)
 {
     if (ctas <= 0) return GPUFFT_SUCCESS;
     if (ctas > 0x7fffffffLL) return GPUFFT_ERROR_INVALID_VALUE;
-    const size_t smem = sizeof(cx<T>) * SMEM_ELEMS;
-    static int smem_done[64] = {0}; // one set per kernel instantiation
-    int st = ensure_smem(pass_kernel<T, FWD, IN, OUT>, smem, smem_done);
-    if (st) return st;
-    pass_kernel<T, FWD, IN, OUT><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
-    return check_launch();
+    const int L = p.L[k];
+    if (k == p.np - 1)
+        return dispatch_int<1, EBITS>(L, [&]<int LL>() { return launch_pass_shape<T, FWD, LL, false>(a, ctas, s); });
+    return dispatch_int<1, 9>(L, [&]<int LL>() { return launch_pass_shape<T, FWD, LL, true>(a, ctas, s); });
 }
 
 } // namespace gfb

@@ -67,91 +67,99 @@ template <typename T> struct FusedArgs
     PassGeo geo;
 };
 
-template <typename T, bool SINGLE>
+// Contiguous pass over both operands: all forward stages of the pass on A and
+// B, the pointwise product, and all inverse stages on the product. SINGLE: the
+// pass is the whole transform (fold + twist in the load, scale + untwist +
+// unfold in the store); otherwise A/B come from and the product returns to the
+// workspace.
+template <typename T, int L, bool SINGLE>
 __global__ void __launch_bounds__(NTHR, 1) fused_kernel(const FusedArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    cx<T>* sx = reinterpret_cast<cx<T>*>(smraw);
-    cx<T>* sy = sx + SMEM_ELEMS;
+    cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+    using S = Sched<0, L>;
+    constexpr int W0 = S::win(0, true), WM = S::win(S::n - 1, true), WE = S::win(S::n - 1, false);
     const int t = threadIdx.x;
     const long long cta = blockIdx.x;
-    const PassGeo& G = a.geo;
-    const long long M = 1LL << G.m;
+    const long long M = 1LL << a.geo.m;
 
+    cx<T> x[2][RPT];
     TwCtx c;
-    c.qoff = 0;
-    c.L = G.L;
-    c.qmask = (1 << G.L) - 1;
-    c.s0 = G.s0;
-    c.neg = 0;
-    c.g = cta_group(G, cta);
-
-    const Rounds Rf = make_rounds(0, G.L, true);
-    const Rounds Ri = make_rounds(0, G.L, false);
-    const int w0 = Rf.lo[0] & ~3;
-
-    cx<T> x[RPT], y[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; r++)
     {
-        const Where w = locate(G, cta, e_of(t, w0, r));
-        if (w.b < a.batch)
+        const Tile<L, false, W0> tl(a.geo, cta, t);
+        c.g = tl.g;
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
         {
-            if (SINGLE)
+            if (tl.b[r] < a.batch)
             {
-                const cx<T> tw = ldg<T>(a.twist + w.j);
-                const T* pa = a.a + w.b * 2 * M + w.j;
-                const T* pb = a.b + w.b * 2 * M + w.j;
-                x[r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
-                y[r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
+                if (SINGLE)
+                {
+                    const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
+                    const T* pa = a.a + tl.b[r] * 2 * M + tl.j[r];
+                    const T* pb = a.b + tl.b[r] * 2 * M + tl.j[r];
+                    x[0][r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
+                    x[1][r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
+                }
+                else
+                {
+                    x[0][r] = a.ws[tl.b[r] * M + tl.j[r]];
+                    x[1][r] = a.ws[(a.batch + tl.b[r]) * M + tl.j[r]];
+                }
             }
             else
             {
-                x[r] = a.ws[w.b * M + w.j];
-                y[r] = a.ws[(a.batch + w.b) * M + w.j];
+                x[0][r] = mk<T>(T(0), T(0));
+                x[1][r] = x[0][r];
             }
         }
-        else
-        {
-            x[r] = mk<T>(T(0), T(0));
-            y[r] = x[r];
-        }
     }
+    c.s0 = a.geo.s0;
+    c.neg = 0;
 
-    run_pass_rounds2<T, true>(x, y, sx, sy, a.roots, c, Rf, t);
+    run_rounds<T, true, 0, L, 2>(x, sm, a.roots, c, t);
+    static_assert(WM == S::win(0, false), "the inverse starts where the forward ends");
+    cx<T> z[1][RPT];
 #pragma unroll
-    for (int r = 0; r < RPT; r++) x[r] = cmul<T>(x[r], y[r]);
-    const int wl = run_pass_rounds<T, false>(x, sx, a.inv_roots, c, Ri, t);
+    for (int r = 0; r < RPT; r++) z[0][r] = cmul<T>(x[0][r], x[1][r]);
+    run_rounds<T, false, 0, L, 1>(z, sm, a.inv_roots, c, t);
 
+    const Tile<L, false, WE> tl(a.geo, cta, t);
 #pragma unroll
     for (int r = 0; r < RPT; r++)
     {
-        const Where w = locate(G, cta, e_of(t, wl, r));
-        if (w.b >= a.batch) continue;
+        if (tl.b[r] >= a.batch) continue;
         if (SINGLE)
         {
-            cx<T> v = cmul<T>(cmul<T>(x[r], mk<T>(a.scale, T(0))), ldg<T>(a.untwist + w.j));
-            T* pc = a.c + w.b * 2 * M + w.j;
+            const cx<T> v = cmul<T>(cmul<T>(z[0][r], mk<T>(a.scale, T(0))), ldg<T>(a.untwist + tl.j[r]));
+            T* pc = a.c + tl.b[r] * 2 * M + tl.j[r];
             st_stream(pc, v.x);
             st_stream(pc + M, v.y);
         }
         else
         {
-            a.ws[w.b * M + w.j] = x[r];
+            a.ws[tl.b[r] * M + tl.j[r]] = z[0][r];
         }
     }
+}
+
+template <typename T, int L, bool SINGLE>
+static int launch_fused_shape(const FusedArgs<T>& a, long long ctas, cudaStream_t s)
+{
+    const size_t smem = 2 * sizeof(cx<T>) * SMEM_ELEMS;
+    static int smem_done[64] = {0};
+    int st = ensure_smem(fused_kernel<T, L, SINGLE>, smem, smem_done);
+    if (st) return st;
+    fused_kernel<T, L, SINGLE><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
+    return check_launch();
 }
 
 template <typename T, bool SINGLE> static int launch_fused(const FusedArgs<T>& a, long long ctas, cudaStream_t s)
 {
     if (ctas <= 0) return GPUFFT_SUCCESS;
     if (ctas > 0x7fffffffLL) return GPUFFT_ERROR_INVALID_VALUE;
-    const size_t smem = 2 * sizeof(cx<T>) * SMEM_ELEMS;
-    static int smem_done[64] = {0};
-    int st = ensure_smem(fused_kernel<T, SINGLE>, smem, smem_done);
-    if (st) return st;
-    fused_kernel<T, SINGLE><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
-    return check_launch();
+    if (!SINGLE) return launch_fused_shape<T, EBITS, false>(a, ctas, s);
+    return dispatch_int<1, EBITS>(a.geo.m, [&]<int LL>() { return launch_fused_shape<T, LL, true>(a, ctas, s); });
 }
 
 constexpr int NATIVE_MIN_NPOWER = 2;
@@ -195,8 +203,6 @@ static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, 
         f.batch = batch;
         f.geo = PassGeo{};
         f.geo.m = m;
-        f.geo.L = m;
-        f.geo.contig = 1;
         const long long ctas = ((long long)batch * M + ECTA - 1) / ECTA;
         return launch_fused<T, true>(f, ctas, s);
     }
@@ -222,7 +228,9 @@ static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, 
             k.table = f.roots;
             k.twist = f.twist;
             k.batch = 2 * w;
-            int st = launch_pass<T, true, IN_FOLD2, OUT_CPX>(k, ctas, s);
+            k.in_kind = IN_FOLD2;
+            k.out_kind = OUT_CPX;
+            int st = launch_pass<T, true>(k, p, 0, ctas, s);
             if (st) return st;
         }
         // 2. last forward pass of both, product, first inverse pass
@@ -246,7 +254,9 @@ static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, 
             k.scale = mk<T>(f.scale, T(0));
             k.do_scale = 1;
             k.batch = w;
-            int st = launch_pass<T, false, IN_CPX, OUT_UNFOLD>(k, ctas, s);
+            k.in_kind = IN_CPX;
+            k.out_kind = OUT_UNFOLD;
+            int st = launch_pass<T, false>(k, p, 0, ctas, s);
             if (st) return st;
         }
     }

@@ -69,6 +69,8 @@ struct SplitArgs
     const cx<float>* twist;
     const cx<float>* untwist;
     unsigned* max_err; // float bits of the largest pre-rounding error (may be null)
+    long long* offs;   // [W][N] exact offset corrections (centred inputs), or null
+    long long K;       // centring offset subtracted from every coefficient (0: none)
     float scale;
     int w, k;
     long long W; // products per wave (stride of the workspace)
@@ -94,62 +96,103 @@ __device__ __forceinline__ void report_err(unsigned* dst, float e)
     if ((threadIdx.x & 31) == 0) atomicMax(dst, __float_as_uint(e));
 }
 
+// Non-negative inputs are centred before they are cut into limbs,
+// a = a' + K u with u = 1 + X + ... + X^(N-1), so that every limb is balanced
+// (a non-centred top limb would make its group values grow like N * mean^2).
+// The product is then
+//     a b = a'b' + K (a'u + b'u) + K^2 uu        (mod X^N + 1)
+// with (x u)_k = 2 P_x(k) - T_x (P = prefix sum, T = total) and (u u)_k =
+// 2k + 2 - N, all exact integers. split_offsets computes
+//     D(k) = 2 (P_a'(k) + P_b'(k)) - T_a' - T_b'
+// for every product of a wave; the recombination adds K D(k) + K^2 (2k+2-N).
+__device__ __forceinline__ long long offset_term(const SplitArgs& a, long long b, long long k, long long N)
+{
+    if (!a.offs) return 0;
+    const long long d = a.offs[b * N + k];
+    return (long long)((unsigned long long)a.K * (unsigned long long)d +
+                       (unsigned long long)a.K * (unsigned long long)a.K * (unsigned long long)(2 * k + 2 - N));
+}
+
+constexpr int OFF_THREADS = 1024;
+
+// One CTA per product: D(k) for k in [0, N) (a block-wide scan of the centred
+// coefficient sums a'_i + b'_i).
+__global__ void __launch_bounds__(OFF_THREADS) split_offsets(const SplitArgs a, int n_power)
+{
+    __shared__ long long part[OFF_THREADS];
+    const long long N = 1LL << n_power;
+    const long long p = blockIdx.x;
+    const int t = threadIdx.x;
+    const long long per = (N + OFF_THREADS - 1) / OFF_THREADS;
+    const long long k0 = t * per;
+    const int32_t* pa = a.a + p * N;
+    const int32_t* pb = a.b + p * N;
+    long long sum = 0;
+    for (long long k = k0; k < k0 + per && k < N; k++) sum += (long long)pa[k] + (long long)pb[k] - 2 * a.K;
+    part[t] = sum;
+    __syncthreads();
+    // inclusive scan of the per-thread sums (Hillis-Steele)
+    for (int off = 1; off < OFF_THREADS; off <<= 1)
+    {
+        const long long v = (t >= off) ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    const long long total = part[OFF_THREADS - 1];
+    long long run = (t > 0) ? part[t - 1] : 0;
+    long long* out = a.offs + p * N;
+    for (long long k = k0; k < k0 + per && k < N; k++)
+    {
+        run += (long long)pa[k] + (long long)pb[k] - 2 * a.K;
+        out[k] = 2 * run - total;
+    }
+}
+
 // --------------------------------------------------------------------------
 // strided first forward pass of every limb polynomial
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(NTHR) split_fwd0(const SplitArgs a)
+template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const SplitArgs a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
+    constexpr int QOFF = EBITS - L;
+    using S = Sched<QOFF, L>;
+    constexpr int W0 = S::win(0, true), WL = S::win(S::n - 1, true);
     const int t = threadIdx.x;
     const long long cta = blockIdx.x;
-    const PassGeo& G = a.geo; // strided, batch index = operand * W + product
-    const long long M = 1LL << G.m;
+    const long long M = 1LL << a.geo.m;
 
-    TwCtx c;
-    c.qoff = G.qoff;
-    c.L = G.L;
-    c.qmask = (1 << G.L) - 1;
-    c.s0 = 0;
-    c.neg = 0;
-    c.g = cta_group(G, cta);
-    const Rounds R = make_rounds(G.qoff, G.L, true);
-    const int w0 = R.lo[0] & ~3;
-
-    // the raw coefficients (fold pair j, j+M) of this CTA's elements
+    // the raw coefficients (fold pair j, j+M) of this CTA's elements, loaded once
+    const Tile<L, true, W0> tl(a.geo, cta, t); // batch index = operand * W + product
+    const long long op = tl.b[0] / a.W, p = tl.b[0] - op * a.W;
+    const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M;
     int vlo[RPT], vhi[RPT];
-    long long jj[RPT];
-    long long bb = 0;
 #pragma unroll
     for (int r = 0; r < RPT; r++)
     {
-        const Where wh = locate(G, cta, e_of(t, w0, r));
-        bb = wh.b;
-        jj[r] = wh.j;
-        const long long op = wh.b / a.W, p = wh.b - op * a.W;
-        const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M + wh.j;
-        vlo[r] = (p < a.batch) ? __ldcs(src) : 0;
-        vhi[r] = (p < a.batch) ? __ldcs(src + M) : 0;
+        vlo[r] = (int)((long long)__ldcs(src + tl.j[r]) - a.K);
+        vhi[r] = (int)((long long)__ldcs(src + tl.j[r] + M) - a.K);
     }
-    const long long op = bb / a.W, p = bb - op * a.W;
+    TwCtx c;
+    c.g = tl.g;
+    c.s0 = 0;
+    c.neg = 0;
+    const Tile<L, true, WL> to(a.geo, cta, t);
     for (int l = 0; l < a.k; l++)
     {
-        cx<float> x[RPT];
+        cx<float> x[1][RPT];
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
             const cx<float> f = mk<float>((float)limb_digit(vlo[r], l, a.w, a.k), (float)limb_digit(vhi[r], l, a.w, a.k));
-            x[r] = cmul<float>(f, ldg<float>(a.twist + jj[r]));
+            x[0][r] = cmul<float>(f, ldg<float>(a.twist + tl.j[r]));
         }
         if (l > 0) __syncthreads();
-        const int wl = run_pass_rounds<float, true>(x, sm, a.roots, c, R, t);
+        run_rounds<float, true, QOFF, L, 1>(x, sm, a.roots, c, t);
         cx<float>* dst = a.spec + ((op * a.k + l) * a.W + p) * M;
 #pragma unroll
-        for (int r = 0; r < RPT; r++)
-        {
-            const Where wh = locate(G, cta, e_of(t, wl, r));
-            if (p < a.batch) dst[wh.j] = x[r];
-        }
+        for (int r = 0; r < RPT; r++) dst[to.j[r]] = x[0][r];
     }
 }
 
@@ -158,107 +201,91 @@ __global__ void __launch_bounds__(NTHR) split_fwd0(const SplitArgs a)
 // first inverse pass of every group (SINGLE: whole transforms, int32 in,
 // int64 out, everything in this kernel)
 // --------------------------------------------------------------------------
-template <bool SINGLE> __global__ void __launch_bounds__(NTHR) split_mid(const SplitArgs a)
+template <int L, bool SINGLE> __global__ void __launch_bounds__(NTHR, 2) split_mid(const SplitArgs a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
+    using S = Sched<0, L>;
+    constexpr int W0 = S::win(0, true), WM = S::win(S::n - 1, true), WE = S::win(S::n - 1, false);
     const int t = threadIdx.x;
     const long long cta = blockIdx.x;
-    const PassGeo& G = a.geo; // contiguous, batch index = product
-    const long long M = 1LL << G.m;
+    const long long M = 1LL << a.geo.m;
 
+    const Tile<L, false, W0> ti(a.geo, cta, t);
+    const Tile<L, false, WM> tm(a.geo, cta, t);
     TwCtx c;
-    c.qoff = 0;
-    c.L = G.L;
-    c.qmask = (1 << G.L) - 1;
-    c.s0 = G.s0;
+    c.g = ti.g;
+    c.s0 = a.geo.s0;
     c.neg = 0;
-    c.g = cta_group(G, cta);
-    const Rounds Rf = make_rounds(0, G.L, true);
-    const Rounds Ri = make_rounds(0, G.L, false);
-    const int w0 = Rf.lo[0] & ~3;
-    const int wl = Ri.lo[0] & ~3; // last forward window == first inverse window
-
-    long long jl[RPT], bl[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; r++)
-    {
-        const Where wh = locate(G, cta, e_of(t, wl, r));
-        jl[r] = wh.j;
-        bl[r] = wh.b;
-    }
 
     // forward last pass of every limb spectrum; results parked in a.spec
     for (int tau = 0; tau < 2 * a.k; tau++)
     {
         const int op = tau / a.k, l = tau - op * a.k;
-        cx<float> x[RPT];
+        cx<float> x[1][RPT];
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            const Where wh = locate(G, cta, e_of(t, w0, r));
-            if (wh.b >= a.batch)
+            if (ti.b[r] >= a.batch)
             {
-                x[r] = mk<float>(0.f, 0.f);
+                x[0][r] = mk<float>(0.f, 0.f);
                 continue;
             }
             if (SINGLE)
             {
-                const int32_t* src = (op == 0 ? a.a : a.b) + wh.b * 2 * M + wh.j;
-                const cx<float> f =
-                    mk<float>((float)limb_digit(__ldg(src), l, a.w, a.k), (float)limb_digit(__ldg(src + M), l, a.w, a.k));
-                x[r] = cmul<float>(f, ldg<float>(a.twist + wh.j));
+                const int32_t* src = (op == 0 ? a.a : a.b) + ti.b[r] * 2 * M + ti.j[r];
+                const long long v0 = (long long)__ldg(src) - a.K, v1 = (long long)__ldg(src + M) - a.K;
+                const cx<float> f = mk<float>((float)limb_digit(v0, l, a.w, a.k), (float)limb_digit(v1, l, a.w, a.k));
+                x[0][r] = cmul<float>(f, ldg<float>(a.twist + ti.j[r]));
             }
             else
             {
-                x[r] = a.spec[((long long)tau * a.W + wh.b) * M + wh.j];
+                x[0][r] = a.spec[((long long)tau * a.W + ti.b[r]) * M + ti.j[r]];
             }
         }
         if (tau > 0) __syncthreads();
-        run_pass_rounds<float, true>(x, sm, a.roots, c, Rf, t);
+        run_rounds<float, true, 0, L, 1>(x, sm, a.roots, c, t);
 #pragma unroll
         for (int r = 0; r < RPT; r++)
-            if (bl[r] < a.batch) a.spec[((long long)tau * a.W + bl[r]) * M + jl[r]] = x[r];
+            if (tm.b[r] < a.batch) a.spec[((long long)tau * a.W + tm.b[r]) * M + tm.j[r]] = x[0][r];
     }
 
     // group sums and the first inverse pass (the whole inverse when SINGLE)
+    static_assert(WM == S::win(0, false), "the inverse starts where the forward ends");
     long long acc_lo[RPT], acc_hi[RPT];
     float err = 0.f;
-    if (SINGLE)
-    {
 #pragma unroll
-        for (int r = 0; r < RPT; r++) acc_lo[r] = acc_hi[r] = 0;
-    }
-    int wend = wl;
+    for (int r = 0; r < RPT; r++) acc_lo[r] = acc_hi[r] = 0;
+    const Tile<L, false, WE> te(a.geo, cta, t);
     for (int s = 0; s <= 2 * (a.k - 1); s++)
     {
         const int i0 = s - (a.k - 1) > 0 ? s - (a.k - 1) : 0;
         const int i1 = s < a.k - 1 ? s : a.k - 1;
-        cx<float> x[RPT];
+        cx<float> x[1][RPT];
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
             cx<float> acc = mk<float>(0.f, 0.f);
-            if (bl[r] < a.batch)
+            if (tm.b[r] < a.batch)
                 for (int i = i0; i <= i1; i++)
                 {
-                    const cx<float> u = a.spec[((long long)i * a.W + bl[r]) * M + jl[r]];
-                    const cx<float> v = a.spec[((long long)(a.k + s - i) * a.W + bl[r]) * M + jl[r]];
+                    const cx<float> u = a.spec[((long long)i * a.W + tm.b[r]) * M + tm.j[r]];
+                    const cx<float> v = a.spec[((long long)(a.k + s - i) * a.W + tm.b[r]) * M + tm.j[r]];
                     acc = cadd<float>(acc, cmul<float>(u, v));
                 }
-            x[r] = acc;
+            x[0][r] = acc;
         }
         __syncthreads();
-        wend = run_pass_rounds<float, false>(x, sm, a.inv_roots, c, Ri, t);
+        run_rounds<float, false, 0, L, 1>(x, sm, a.inv_roots, c, t);
         if (SINGLE)
         {
             const int sh = a.w * s;
 #pragma unroll
             for (int r = 0; r < RPT; r++)
             {
-                const Where wh = locate(G, cta, e_of(t, wend, r));
-                if (wh.b >= a.batch) continue;
-                const cx<float> v = cmul<float>(cmul<float>(x[r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + wh.j));
+                if (te.b[r] >= a.batch) continue;
+                const cx<float> v =
+                    cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j[r]));
                 const float rr = rintf(v.x), ri = rintf(v.y);
                 err = fmaxf(err, group_error(v, rr, ri));
                 acc_lo[r] += (long long)((unsigned long long)(long long)rr << sh);
@@ -270,10 +297,7 @@ template <bool SINGLE> __global__ void __launch_bounds__(NTHR) split_mid(const S
             cx<float>* dst = a.group + (long long)s * a.W * M;
 #pragma unroll
             for (int r = 0; r < RPT; r++)
-            {
-                const Where wh = locate(G, cta, e_of(t, wend, r));
-                if (wh.b < a.batch) dst[wh.b * M + wh.j] = x[r];
-            }
+                if (te.b[r] < a.batch) dst[te.b[r] * M + te.j[r]] = x[0][r];
         }
     }
     if (SINGLE)
@@ -281,11 +305,10 @@ template <bool SINGLE> __global__ void __launch_bounds__(NTHR) split_mid(const S
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            const Where wh = locate(G, cta, e_of(t, wend, r));
-            if (wh.b >= a.batch) continue;
-            int64_t* dst = a.c + wh.b * 2 * M + wh.j;
-            __stcs(reinterpret_cast<long long*>(dst), acc_lo[r]);
-            __stcs(reinterpret_cast<long long*>(dst + M), acc_hi[r]);
+            if (te.b[r] >= a.batch) continue;
+            int64_t* dst = a.c + te.b[r] * 2 * M + te.j[r];
+            __stcs(reinterpret_cast<long long*>(dst), acc_lo[r] + offset_term(a, te.b[r], te.j[r], 2 * M));
+            __stcs(reinterpret_cast<long long*>(dst + M), acc_hi[r] + offset_term(a, te.b[r], te.j[r] + M, 2 * M));
         }
         report_err(a.max_err, err);
     }
@@ -294,63 +317,55 @@ template <bool SINGLE> __global__ void __launch_bounds__(NTHR) split_mid(const S
 // --------------------------------------------------------------------------
 // strided last inverse pass of every group, rounding and int64 recombination
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(NTHR) split_inv0(const SplitArgs a)
+template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitArgs a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
+    constexpr int QOFF = EBITS - L;
+    using S = Sched<QOFF, L>;
+    constexpr int W0 = S::win(0, false), WE = S::win(S::n - 1, false);
     const int t = threadIdx.x;
     const long long cta = blockIdx.x;
-    const PassGeo& G = a.geo; // strided, batch index = product
-    const long long M = 1LL << G.m;
+    const long long M = 1LL << a.geo.m;
 
+    const Tile<L, true, W0> ti(a.geo, cta, t); // batch index = product
+    const Tile<L, true, WE> te(a.geo, cta, t);
     TwCtx c;
-    c.qoff = G.qoff;
-    c.L = G.L;
-    c.qmask = (1 << G.L) - 1;
+    c.g = ti.g;
     c.s0 = 0;
     c.neg = 0;
-    c.g = cta_group(G, cta);
-    const Rounds R = make_rounds(G.qoff, G.L, false);
-    const int w0 = R.lo[0] & ~3;
+    const long long p = ti.b[0];
 
     long long acc_lo[RPT], acc_hi[RPT];
 #pragma unroll
     for (int r = 0; r < RPT; r++) acc_lo[r] = acc_hi[r] = 0;
     float err = 0.f;
-    int wend = w0;
     for (int s = 0; s <= 2 * (a.k - 1); s++)
     {
-        const cx<float>* src = a.group + (long long)s * a.W * M;
-        cx<float> x[RPT];
+        const cx<float>* src = a.group + ((long long)s * a.W + p) * M;
+        cx<float> x[1][RPT];
 #pragma unroll
-        for (int r = 0; r < RPT; r++)
-        {
-            const Where wh = locate(G, cta, e_of(t, w0, r));
-            x[r] = (wh.b < a.batch) ? src[wh.b * M + wh.j] : mk<float>(0.f, 0.f);
-        }
+        for (int r = 0; r < RPT; r++) x[0][r] = src[ti.j[r]];
         if (s > 0) __syncthreads();
-        wend = run_pass_rounds<float, false>(x, sm, a.inv_roots, c, R, t);
+        run_rounds<float, false, QOFF, L, 1>(x, sm, a.inv_roots, c, t);
         const int sh = a.w * s;
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            const Where wh = locate(G, cta, e_of(t, wend, r));
-            if (wh.b >= a.batch) continue;
-            const cx<float> v = cmul<float>(cmul<float>(x[r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + wh.j));
+            const cx<float> v =
+                cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j[r]));
             const float rr = rintf(v.x), ri = rintf(v.y);
             err = fmaxf(err, group_error(v, rr, ri));
             acc_lo[r] += (long long)((unsigned long long)(long long)rr << sh);
             acc_hi[r] += (long long)((unsigned long long)(long long)ri << sh);
         }
     }
+    int64_t* dst = a.c + p * 2 * M;
 #pragma unroll
     for (int r = 0; r < RPT; r++)
     {
-        const Where wh = locate(G, cta, e_of(t, wend, r));
-        if (wh.b >= a.batch) continue;
-        int64_t* dst = a.c + wh.b * 2 * M + wh.j;
-        __stcs(reinterpret_cast<long long*>(dst), acc_lo[r]);
-        __stcs(reinterpret_cast<long long*>(dst + M), acc_hi[r]);
+        __stcs(reinterpret_cast<long long*>(dst + te.j[r]), acc_lo[r] + offset_term(a, p, te.j[r], 2 * M));
+        __stcs(reinterpret_cast<long long*>(dst + te.j[r] + M), acc_hi[r] + offset_term(a, p, te.j[r] + M, 2 * M));
     }
     report_err(a.max_err, err);
 }
@@ -358,20 +373,22 @@ __global__ void __launch_bounds__(NTHR) split_inv0(const SplitArgs a)
 // --------------------------------------------------------------------------
 // host side
 // --------------------------------------------------------------------------
-// Largest pre-rounding error expected for k limbs of width w at ring size N.
+// Largest pre-rounding error expected for k balanced limbs of width w.
 // For one limb pair the measured maximum over a batch follows
 //     err ~ C * rms(d_a) * rms(d_b) * sqrt(N) * sqrt(log2(N/2)) * 2^-24,  C = 7.1
 // (calibrated on FP32 negacyclic limb products: balanced 6-bit limbs at
 // N = 2^16 give 0.144). A group sum of several pairs adds their errors in
-// quadrature. Balanced digits have rms 2^(w-1)/sqrt(3); the top digit holds the
-// tb = input_bits - w(k-1) leftover bits: rms 0.577 * 2^tb when the inputs are
-// non-negative (digit in [0, 2^tb]), 2^tb / sqrt(3) when signed.
-static double predicted_error(int n_power, int input_bits, int w, int k, bool non_negative)
+// quadrature. The coefficients are signed values of magnitude below 2^B
+// (B = input_bits, or input_bits - 1 after centring non-negative inputs);
+// digits have rms 2^(w-1)/sqrt(3), the top digit 2^tb/sqrt(3) with
+// tb = B - w(k-1) leftover bits. Also returns the typical largest group value
+// (4 sigma) through *mag.
+static double predicted_error(int n_power, int B, int w, int k, double* mag)
 {
     double r[SPLIT_MAX_LIMBS];
     for (int l = 0; l < k; l++) r[l] = std::ldexp(1.0, w - 1) / std::sqrt(3.0);
-    const int tb = input_bits - w * (k - 1);
-    r[k - 1] = non_negative ? 0.577 * std::ldexp(1.0, tb) : std::ldexp(1.0, tb) / std::sqrt(3.0);
+    const int tb = B - w * (k - 1);
+    r[k - 1] = std::ldexp(1.0, tb) / std::sqrt(3.0);
     double worst = 0.0;
     for (int s = 0; s <= 2 * (k - 1); s++)
     {
@@ -383,17 +400,22 @@ static double predicted_error(int n_power, int input_bits, int w, int k, bool no
         }
         worst = std::max(worst, std::sqrt(e2));
     }
-    return 7.1 * worst * std::sqrt(std::ldexp(1.0, n_power)) * std::sqrt((double)(n_power - 1)) * std::ldexp(1.0, -24);
+    const double sqn = std::sqrt(std::ldexp(1.0, n_power));
+    if (mag) *mag = 4.0 * worst * sqn;
+    return 7.1 * worst * sqn * std::sqrt((double)(n_power - 1)) * std::ldexp(1.0, -24);
 }
 
 static bool choose_limbs(int n_power, int input_bits, bool non_negative, int* w_out, int* k_out)
 {
-    // the plan with the fewest limbs whose predicted error is at most 0.2
+    // the plan with the fewest limbs whose predicted error is at most 0.2 and
+    // whose group values stay far inside FP32's certifiable range (< 2^21)
+    const int B = non_negative ? input_bits - 1 : input_bits;
     for (int k = 1; k <= SPLIT_MAX_LIMBS; k++)
     {
-        const int w = (input_bits + k - 1) / k;
-        if (w < 1 || w > 20) continue;
-        if (predicted_error(n_power, input_bits, w, k, non_negative) <= 0.2)
+        const int w = (B + 1 + k - 1) / k; // k balanced digits of w bits cover 2^B in magnitude
+        if (w < 1 || w > 20 || B - w * (k - 1) > w - 1) continue;
+        double mag = 0;
+        if (predicted_error(n_power, B, w, k, &mag) <= 0.2 && mag < std::ldexp(1.0, 21))
         {
             *w_out = w;
             *k_out = k;
@@ -405,15 +427,18 @@ static bool choose_limbs(int n_power, int input_bits, bool non_negative, int* w_
 
 static long long split_wave(int m, int k, long long batch)
 {
-    const size_t per = (size_t)(4 * k - 1) * ((size_t)1 << m) * sizeof(cx<float>);
+    const size_t per = (size_t)(4 * k - 1) * ((size_t)1 << m) * sizeof(cx<float>) + ((size_t)2 << m) * 8;
     long long w = (long long)((64ull << 20) / per);
     if (w < 1) w = 1;
     return w < batch ? w : batch;
 }
 
+// [2k limb spectra | 2k-1 group spectra] of W products (complex float, M each)
+// followed by W x N int64 offset corrections
 static size_t split_ws_bytes(int m, int k, long long W)
 {
-    return (size_t)(4 * k - 1) * (size_t)W * ((size_t)1 << m) * sizeof(cx<float>);
+    return (size_t)(4 * k - 1) * (size_t)W * ((size_t)1 << m) * sizeof(cx<float>) +
+           (size_t)W * ((size_t)2 << m) * sizeof(long long);
 }
 
 template <typename K> static int launch_split(K* kern, int* done, const SplitArgs& a, long long ctas, cudaStream_t s)
@@ -425,6 +450,22 @@ template <typename K> static int launch_split(K* kern, int* done, const SplitArg
     if (st) return st;
     kern<<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
     return check_launch();
+}
+
+template <int L, bool SINGLE> static int launch_mid(const SplitArgs& a, long long ctas, cudaStream_t s)
+{
+    static int done[64] = {0};
+    return launch_split(split_mid<L, SINGLE>, done, a, ctas, s);
+}
+template <int L> static int launch_fwd0(const SplitArgs& a, long long ctas, cudaStream_t s)
+{
+    static int done[64] = {0};
+    return launch_split(split_fwd0<L>, done, a, ctas, s);
+}
+template <int L> static int launch_inv0(const SplitArgs& a, long long ctas, cudaStream_t s)
+{
+    static int done[64] = {0};
+    return launch_split(split_inv0<L>, done, a, ctas, s);
 }
 
 static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch, int input_bits,
@@ -441,6 +482,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         if (!choose_limbs(n_power, input_bits, non_negative != 0, &w, &k)) return GPUFFT_ERROR_INVALID_VALUE;
     }
     if (k > SPLIT_MAX_LIMBS || w < 1 || w > 20 || (long long)w * k < input_bits) return GPUFFT_ERROR_INVALID_VALUE;
+    if (non_negative && input_bits > 30) return GPUFFT_ERROR_INVALID_VALUE;
 
     const int m = n_power - 1;
     const long long M = 1LL << m;
@@ -456,6 +498,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
     A.scale = (float)(1.0 / (double)M);
     A.w = w;
     A.k = k;
+    A.K = non_negative ? (1LL << (input_bits - 1)) : 0;
 
     long long W = split_wave(m, k, batch);
     const size_t need1 = split_ws_bytes(m, k, 1);
@@ -466,7 +509,6 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         cudaError_t e = cudaMemsetAsync(max_err, 0, sizeof(unsigned), s);
         if (e != cudaSuccess) return set_cuda_error(e);
     }
-    static int done_mid1[64] = {0}, done_mid0[64] = {0}, done_f0[64] = {0}, done_i0[64] = {0};
     const Plan p = make_plan(m);
     for (long long p0 = 0; p0 < batch; p0 += W)
     {
@@ -478,26 +520,33 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         A.batch = wv;
         A.spec = reinterpret_cast<cx<float>*>(ws);
         A.group = A.spec + (size_t)(2 * k) * wv * M;
+        A.offs = nullptr;
+        if (A.K)
+        {
+            A.offs = reinterpret_cast<long long*>(A.group + (size_t)(2 * k - 1) * wv * M);
+            split_offsets<<<(unsigned)wv, OFF_THREADS, 0, s>>>(A, n_power);
+            const int st = check_launch();
+            if (st) return st;
+        }
         if (m <= EBITS)
         {
             A.geo = PassGeo{};
             A.geo.m = m;
-            A.geo.L = m;
-            A.geo.contig = 1;
             const long long ctas = (wv * M + ECTA - 1) / ECTA;
-            int st = launch_split(split_mid<true>, done_mid1, A, ctas, s);
+            int st = dispatch_int<1, EBITS>(m, [&]<int LL>() { return launch_mid<LL, true>(A, ctas, s); });
             if (st) return st;
             continue;
         }
         long long ctas = 0;
+        const int L0 = p.L[0];
         A.geo = pass_geo(p, 0, m, 0, 2 * wv, &ctas);
-        int st = launch_split(split_fwd0, done_f0, A, ctas, s);
+        int st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_fwd0<LL>(A, ctas, s); });
         if (st) return st;
         A.geo = pass_geo(p, 1, m, 0, wv, &ctas);
-        st = launch_split(split_mid<false>, done_mid0, A, ctas, s);
+        st = launch_mid<EBITS, false>(A, ctas, s);
         if (st) return st;
         A.geo = pass_geo(p, 0, m, 0, wv, &ctas);
-        st = launch_split(split_inv0, done_i0, A, ctas, s);
+        st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_inv0<LL>(A, ctas, s); });
         if (st) return st;
     }
     return GPUFFT_SUCCESS;

@@ -55,9 +55,9 @@ def test_split_config3_full_batch(gf, O, dev):
 
 
 def test_split_reports_inexact_plan(gf, dev):
-    # an under-sized limb plan (one 24-bit limb) is flagged by the error report
+    # an under-sized limb plan (two 12-bit limbs) is flagged by the error report
     rng = np.random.default_rng(9)
     n = 1 << 14
     a = torch.from_numpy(rng.integers(0, 1 << 24, (1, n)).astype(np.int32)).to(dev)
-    _, err = gf.negacyclic_mul_split(a, a, input_bits=24, non_negative=True, limbs=(24, 1), return_error=True)
+    _, err = gf.negacyclic_mul_split(a, a, input_bits=24, non_negative=True, limbs=(12, 2), return_error=True)
     assert float(err.item()) >= 0.5
