@@ -78,6 +78,7 @@ def lib() -> ctypes.CDLL:
         L.gpufft_negacyclic_mul_workspace_bytes.restype = sz
         L.gpufft_negacyclic_mul_f32.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
         L.gpufft_negacyclic_mul_f64.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
+        L.gpufft_negacyclic_mul_f64_noalloc.argtypes = [vp, vp, vp, i, i, vp, vp]
         L.gpufft_host_fft_tables_f32.argtypes = [i, vp, vp, vp]
         L.gpufft_host_fft_tables_f64.argtypes = [i, vp, vp, vp]
         L.gpufft_host_ffnt_tables_f32.argtypes = [i, vp, vp, vp, vp]

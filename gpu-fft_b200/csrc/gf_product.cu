@@ -319,3 +319,70 @@ extern "C" int gpufft_negacyclic_mul_f64(const double* a, const double* b, doubl
     return gfb::negacyclic_mul<double>(a, b, c, n_power, batch, tables, workspace, workspace_bytes,
                                        (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of gpufft_negacyclic_mul_f64.
+//
+// Some callers cannot call cudaMalloc at all: code running where the CUDA
+// allocator is off limits (inside a foreign runtime's memory pool, a plugin
+// host that owns every device allocation, or a process that must not grow its
+// device footprint after start-up), and callers that only hold the buffers
+// they were handed. For them this entry point takes its scratch from a
+// library-owned, file-scope device array instead of a caller workspace.
+//
+// * The array is NOALLOC_SCRATCH_BYTES (16 MiB). It is part of this module's
+//   device image, so every GPU on which the library's kernels are loaded holds
+//   it until the process exits.
+// * Host code may not use the array's name as a device address (on the host it
+//   names a host-side shadow). The device address is looked up with
+//   cudaGetSymbolAddress once per device, on the first call made on that
+//   device, with that device current; make that first call before any stream
+//   capture.
+// * Rings whose one-product workspace exceeds the array (N > 2^20) are
+//   rejected with GPUFFT_ERROR_WORKSPACE. Larger batches run in more waves.
+// * All calls share the array and nothing in it needs to start at zero (every
+//   byte a wave reads was written earlier in the same wave). Calls whose work
+//   overlaps on the GPU (different streams, or different host threads without
+//   ordering) race on the array: serialise them.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace gfb
+{
+constexpr size_t NOALLOC_SCRATCH_BYTES = 16ull << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+static int noalloc_scratch(void** out)
+{
+    static std::mutex mu;
+    static void* addr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    if (dev < 0 || dev >= 64) return set_cuda_error(cudaErrorInvalidDevice);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev])
+    {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return GPUFFT_SUCCESS;
+}
+} // namespace gfb
+
+extern "C" int gpufft_negacyclic_mul_f64_noalloc(const double* a, const double* b, double* c, int n_power,
+                                                 int batch, const void* tables, gpufft_stream_t stream)
+{
+    if (n_power < gfb::NATIVE_MIN_NPOWER || n_power > gfb::NATIVE_MAX_NPOWER) return GPUFFT_ERROR_INVALID_N_POWER;
+    const int m = n_power - 1;
+    if (m > gfb::EBITS && 2 * ((size_t)1 << m) * sizeof(double2) > gfb::NOALLOC_SCRATCH_BYTES)
+        return GPUFFT_ERROR_WORKSPACE;
+    void* scratch = nullptr;
+    int st = gfb::noalloc_scratch(&scratch);
+    if (st) return st;
+    return gfb::negacyclic_mul<double>(a, b, c, n_power, batch, tables, scratch, gfb::NOALLOC_SCRATCH_BYTES,
+                                       (cudaStream_t)stream);
+}

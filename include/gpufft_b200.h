@@ -149,6 +149,17 @@ int gpufft_negacyclic_mul_f64(const double* a, const double* b, double* c, int n
                               const void* tables, void* workspace, size_t workspace_bytes,
                               gpufft_stream_t stream);
 
+/* Allocation-free gpufft_negacyclic_mul_f64, for callers that cannot call
+ * cudaMalloc (code running inside another runtime's device memory pool, plugin
+ * hosts that own every device allocation, processes that must not grow their
+ * device footprint after start-up). No reference counterpart. Scratch is a
+ * 16 MiB library-owned device array that every GPU loading the library holds
+ * until exit; the first call on each device looks up its address, so make it
+ * before any stream capture. Rings with N > 2^20 return GPUFFT_ERROR_WORKSPACE.
+ * All calls share the array: calls that overlap on the GPU race on it. */
+int gpufft_negacyclic_mul_f64_noalloc(const double* a, const double* b, double* c, int n_power, int batch,
+                                      const void* tables, gpufft_stream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* FP32 split-precision negacyclic product with exact int64 output (no      */
 /* reference counterpart: the reference's products are plain FP32/FP64).     */
