@@ -39,7 +39,10 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64"], default="split")
+    p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64", "batch", "vjp"], default="split",
+                   help="split/f64/f32/dropin_f64: config 3 (N = 2^16 negacyclic products); "
+                        "batch: config 4 (4096 mixed ring sizes 2^10..2^17, one persistent launch in a CUDA "
+                        "graph); vjp: config 5 (FP32 linear convolution N = 2^14, batch 512, forward + VJP)")
     p.add_argument("--no-compare", dest="compare", action="store_false",
                    help="time only --path (by default FP64 is timed beside it)")
     p.add_argument("--n-power", type=int, default=16)
@@ -262,6 +265,182 @@ def time_path(step, a, b, c, hosts, args, stream, torch, barrier, max_over_ranks
     return ms, ms_e2e, t0, t1
 
 
+def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, peak, peak_kind):
+    """Config 4: 4096 negacyclic products, ring sizes log-uniform over 2^10..2^17,
+    coefficients in [-2^15, 2^15), FP64, one persistent launch replayed from a
+    CUDA graph; per-size sequential launches timed beside it."""
+    import numpy as np
+    rng = np.random.default_rng(SEED + 1 + rank)
+    n_powers = [int(x) for x in rng.integers(10, 18, 4096)]
+    plan = gf.BatchPlan(n_powers, torch.float64)
+    g = torch.Generator().manual_seed(SEED + 1 + rank)
+    a_host = torch.randint(-(1 << 15), 1 << 15, (plan.total,), generator=g).double().pin_memory()
+    b_host = torch.randint(-(1 << 15), 1 << 15, (plan.total,), generator=g).double().pin_memory()
+    c_host = torch.empty_like(a_host).pin_memory()
+    a, b = a_host.to(dev), b_host.to(dev)
+    c = torch.empty_like(a)
+    plan.autotune(a, b, c, os.path.join(ROOT, "gpu-fft_b200", "lib", "batch_autotune.jsonl"))
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    plan.capture(a, b, c, s)
+    # per-size sequential reference path (same data, one call per ring size)
+    sizes = sorted(set(n_powers))
+    offs = plan.offsets
+    groups = []
+    for np_ in sizes:
+        idx = [i for i, n in enumerate(n_powers) if n == np_]
+        o0 = int(min(offs[i] for i in idx))
+        groups.append((np_, len(idx), o0))
+    tabs = {np_: gf.ffnt_tables(np_, "f64", dev) for np_ in sizes}
+    wss = {np_: torch.empty(max(1, gf.negacyclic_mul_workspace_bytes(np_, cnt, 64)), dtype=torch.uint8, device=dev)
+           for np_, cnt, _ in groups}
+
+    def seq_step(out):
+        for np_, cnt, o0 in groups:
+            n = 1 << np_
+            gf.negacyclic_mul(a[o0:o0 + cnt * n].view(cnt, n), b[o0:o0 + cnt * n].view(cnt, n),
+                              out=out[o0:o0 + cnt * n].view(cnt, n), tables=tabs[np_], workspace=wss[np_],
+                              stream=s)
+    with torch.cuda.stream(s):
+        with clk_cls(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+            time.sleep(0.5)
+            for _ in range(args.warmup):
+                plan.replay(s)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.time()
+            e0.record(s)
+            for _ in range(args.steps):
+                plan.replay(s)
+            e1.record(s)
+            barrier()
+            t1 = time.time()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        c_seq = torch.empty_like(a)
+        for _ in range(args.warmup):
+            seq_step(c_seq)
+        barrier()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(s)
+        for _ in range(args.steps):
+            seq_step(c_seq)
+        e3.record(s)
+        barrier()
+        ms_seq = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+        identical = bool(torch.equal(c, c_seq))
+        # end to end: host operands in, host products out, every step
+        for _ in range(max(1, args.warmup // 2)):
+            a.copy_(a_host, non_blocking=True)
+            b.copy_(b_host, non_blocking=True)
+            plan.replay(s)
+            c_host.copy_(c, non_blocking=True)
+        barrier()
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record(s)
+        for _ in range(args.steps):
+            a.copy_(a_host, non_blocking=True)
+            b.copy_(b_host, non_blocking=True)
+            plan.replay(s)
+            c_host.copy_(c, non_blocking=True)
+        e5.record(s)
+        barrier()
+        ms_e2e = max_over_ranks(e4.elapsed_time(e5) / args.steps)
+    alg = 3 * plan.total * 8
+    achieved = alg / (ms * 1e-3) / 1e9
+    info = plan.info()
+    line = {
+        "metric": "negacyclic poly-mults/s, 4096 mixed ring sizes 2^10..2^17", "value": world * 4096 / (ms * 1e-3),
+        "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, log-uniform ring sizes, coefficients uniform in [-2^15, 2^15))",
+        "config": {"workload": "4096 negacyclic products, ring sizes log-uniform 2^10..2^17, FP64, one persistent "
+                               "cooperative launch replayed from a CUDA graph", "requests": 4096,
+                   "coefficients": plan.total, "launch_shape": info, "l2": "inputs larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_step": alg,
+                     "timed": "graph replay of the persistent launch, CUDA events"},
+        "e2e": {"value": world * 4096 / (ms_e2e * 1e-3), "unit": "products/s", "h2d_bytes_per_step": 2 * alg // 3,
+                "d2h_bytes_per_step": alg // 3},
+        "per_size_sequential": {"value": world * 4096 / (ms_seq * 1e-3), "unit": "products/s", "ms_per_step": ms_seq,
+                                "identical_outputs": identical},
+        "gpu_launches": args.steps, "clocks": clk.summary(t0, t1),
+    }
+    plan.close()
+    return line
+
+
+def run_vjp(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, peak, peak_kind):
+    """Config 5: FP32 linear convolution N = 2^14 (zero-padded to 2^15), batch
+    512; a step is the forward product plus the VJP for both operands."""
+    n, batch = 1 << 14, 512
+    g = torch.Generator().manual_seed(SEED + 2 + rank)
+    a_host = torch.randn((batch, n), generator=g).pin_memory()
+    b_host = torch.randn((batch, n), generator=g).pin_memory()
+    g_host = torch.randn((batch, 2 * n), generator=g).pin_memory()
+    outs_host = [torch.empty((batch, n)).pin_memory(), torch.empty((batch, n)).pin_memory(),
+                 torch.empty((batch, 2 * n)).pin_memory()]
+    a, b, gr = a_host.to(dev), b_host.to(dev), g_host.to(dev)
+    tables = gf.ffnt_tables(15, "f32", dev)
+    ws_f = torch.empty(max(1, int(gf.lib().gpufft_linear_mul_workspace_bytes(14, batch, 32))), dtype=torch.uint8,
+                       device=dev)
+    ws_b = torch.empty(max(1, int(gf.lib().gpufft_linear_mul_vjp_workspace_bytes(14, batch))), dtype=torch.uint8,
+                       device=dev)
+    c = torch.empty((batch, 2 * n), device=dev)
+    ga, gb = torch.empty_like(a), torch.empty_like(b)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        gf.linear_mul(a, b, out=c, tables=tables, workspace=ws_f)
+        gf.linear_mul_vjp(gr, a, b, grad_a=ga, grad_b=gb, tables=tables, workspace=ws_b)
+    with clk_cls(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        time.sleep(0.5)
+        for _ in range(args.warmup):
+            step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.time()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        barrier()
+        t1 = time.time()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    for _ in range(max(1, args.warmup // 2)):
+        step()
+    barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        a.copy_(a_host, non_blocking=True)
+        b.copy_(b_host, non_blocking=True)
+        gr.copy_(g_host, non_blocking=True)
+        step()
+        outs_host[0].copy_(ga, non_blocking=True)
+        outs_host[1].copy_(gb, non_blocking=True)
+        outs_host[2].copy_(c, non_blocking=True)
+    e3.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+    # forward: a, b in (2N*4 bytes), c out (2N*4); backward: g (2N*4), a, b in, grads out (2N*4)
+    alg = batch * (4 * n * 4 + 6 * n * 4)
+    achieved = alg / (ms * 1e-3) / 1e9
+    return {
+        "metric": "forward+backward linear-convolution products/s (N=2^14, FP32)",
+        "value": world * batch / (ms * 1e-3), "unit": "products/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded i.i.d. N(0,1))",
+        "config": {"workload": "real FP32 linear convolution N=2^14 zero-padded to 2^15, batch 512, forward + VJP",
+                   "batch_per_gpu": batch, "l2": "inputs larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_step": alg,
+                     "timed": "forward product + VJP per step, CUDA events"},
+        "e2e": {"value": world * batch / (ms_e2e * 1e-3), "unit": "products/s",
+                "h2d_bytes_per_step": batch * 4 * n * 4, "d2h_bytes_per_step": batch * 4 * n * 4},
+        "gpu_launches": 6 * args.steps, "clocks": clk.summary(t0, t1),
+    }
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -300,6 +479,15 @@ def main():
         return float(t.item())
 
     peak, peak_kind = peaks()
+    if args.path in ("batch", "vjp"):
+        fn = run_batch if args.path == "batch" else run_vjp
+        line = fn(args, gf, dev, torch, world, rank, barrier, max_over_ranks, ClockSampler, peak, peak_kind)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     results = {}
     paths = [args.path] + ([p for p in ("f64",) if p != args.path] if args.compare else [])
     with ClockSampler(local) as clk:

@@ -83,6 +83,26 @@ def lib() -> ctypes.CDLL:
         L.gpufft_host_fft_tables_f64.argtypes = [i, vp, vp, vp]
         L.gpufft_host_ffnt_tables_f32.argtypes = [i, vp, vp, vp, vp]
         L.gpufft_host_ffnt_tables_f64.argtypes = [i, vp, vp, vp, vp]
+        L.gpufft_linear_mul_workspace_bytes.argtypes = [i, i, i]
+        L.gpufft_linear_mul_workspace_bytes.restype = sz
+        L.gpufft_linear_mul_f32.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
+        L.gpufft_linear_mul_f64.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
+        L.gpufft_linear_mul_vjp_workspace_bytes.argtypes = [i, i]
+        L.gpufft_linear_mul_vjp_workspace_bytes.restype = sz
+        L.gpufft_linear_mul_vjp_f32.argtypes = [vp, vp, vp, vp, vp, i, i, vp, vp, sz, vp]
+        ll = ctypes.c_longlong
+        vpp = ctypes.POINTER(ctypes.c_void_p)
+        L.gpufft_batch_plan_create.argtypes = [vpp, ctypes.POINTER(ctypes.c_int), i, i, vp]
+        L.gpufft_batch_plan_layout.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ll),
+                                               ctypes.POINTER(ll)]
+        L.gpufft_batch_plan_execute.argtypes = [vp, vp, vp, vp, vp]
+        L.gpufft_batch_plan_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_char_p, vp]
+        L.gpufft_batch_plan_capture.argtypes = [vp, vp, vp, vp, vp]
+        L.gpufft_batch_plan_replay.argtypes = [vp, vp]
+        L.gpufft_batch_plan_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ll)]
+        L.gpufft_batch_plan_status.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+        L.gpufft_batch_plan_destroy.argtypes = [vp]
         ip = ctypes.POINTER(ctypes.c_int)
         L.gpufft_split_plan.argtypes = [i, i, i, ip, ip]
         L.gpufft_negacyclic_mul_split_workspace_bytes.argtypes = [i, i, i]
@@ -293,3 +313,134 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
         _stream_handle(stream))
     check(st, "negacyclic_mul_split")
     return (out, err) if return_error else out
+
+
+def linear_mul(a, b, out=None, tables=None, workspace=None, stream=None):
+    """Linear product of the rows of (batch, N) float tensors: (batch, 2N) result
+    (the R_R product, computed with half-length transforms). Not rounded."""
+    import torch
+    batch, n = a.shape
+    n_power = n.bit_length() - 1
+    if (1 << n_power) != n or b.shape != a.shape or a.dtype != b.dtype:
+        raise GpufftError(ERROR_INVALID_VALUE, "a and b must be (batch, 2^k) tensors of one dtype")
+    f64 = a.dtype == torch.float64
+    if tables is None:
+        tables = ffnt_tables(n_power + 1, "f64" if f64 else "f32", a.device, stream)
+    if out is None:
+        out = torch.empty((batch, 2 * n), dtype=a.dtype, device=a.device)
+    need = int(lib().gpufft_linear_mul_workspace_bytes(n_power, batch, 64 if f64 else 32))
+    if workspace is None and need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=a.device)
+    ws_ptr = workspace.data_ptr() if workspace is not None else None
+    ws_len = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    f = lib().gpufft_linear_mul_f64 if f64 else lib().gpufft_linear_mul_f32
+    check(f(_ptr(a), _ptr(b), _ptr(out), n_power, batch, _ptr(tables), ws_ptr, ws_len, _stream_handle(stream)),
+          "linear_mul")
+    return out
+
+
+def linear_mul_vjp(g, a, b, grad_a=None, grad_b=None, tables=None, workspace=None, stream=None):
+    """Adjoint of linear_mul (float32): for the upstream gradient g (batch, 2N),
+    returns (grad_a, grad_b), each (batch, N)."""
+    import torch
+    batch, n = a.shape
+    n_power = n.bit_length() - 1
+    if tables is None:
+        tables = ffnt_tables(n_power + 1, "f32", a.device, stream)
+    if grad_a is None:
+        grad_a = torch.empty_like(a)
+    if grad_b is None:
+        grad_b = torch.empty_like(b)
+    need = int(lib().gpufft_linear_mul_vjp_workspace_bytes(n_power, batch))
+    if workspace is None and need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=a.device)
+    ws_ptr = workspace.data_ptr() if workspace is not None else None
+    ws_len = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    check(lib().gpufft_linear_mul_vjp_f32(_ptr(g), _ptr(a), _ptr(b), _ptr(grad_a), _ptr(grad_b), n_power, batch,
+                                          _ptr(tables), ws_ptr, ws_len, _stream_handle(stream)), "linear_mul_vjp")
+    return grad_a, grad_b
+
+
+class BatchPlan:
+    """Negacyclic products of mixed ring sizes in one persistent launch.
+
+    plan = BatchPlan(n_powers, torch.float64)
+    a_packed = plan.pack([a_0, a_1, ...])          # requests grouped by size
+    c_packed = plan.execute(a_packed, b_packed)   # or capture() once, replay() after
+    c_list = plan.unpack(c_packed)
+    """
+
+    def __init__(self, n_powers, dtype, stream=None):
+        import numpy as np
+        import torch
+        self.n_powers = [int(x) for x in n_powers]
+        self.dtype = dtype
+        self.bits = 64 if dtype == torch.float64 else 32
+        arr = (ctypes.c_int * len(self.n_powers))(*self.n_powers)
+        h = ctypes.c_void_p()
+        check(lib().gpufft_batch_plan_create(ctypes.byref(h), arr, len(self.n_powers), self.bits,
+                                             _stream_handle(stream)), "batch_plan_create")
+        self.h = h
+        n = len(self.n_powers)
+        order = (ctypes.c_int * n)()
+        offs = (ctypes.c_longlong * n)()
+        total = ctypes.c_longlong()
+        check(lib().gpufft_batch_plan_layout(self.h, order, offs, ctypes.byref(total)), "batch_plan_layout")
+        self.order = np.array(order[:], dtype=np.int64)
+        self.offsets = np.array(offs[:], dtype=np.int64)
+        self.total = int(total.value)
+
+    def pack(self, polys):
+        """Concatenate per-request rows (length 2^n_powers[i]) in the plan's layout."""
+        import torch
+        out = torch.empty(self.total, dtype=self.dtype, device=polys[0].device)
+        for i, p in enumerate(polys):
+            o = int(self.offsets[i])
+            out[o: o + p.numel()].copy_(p.reshape(-1))
+        return out
+
+    def unpack(self, packed):
+        return [packed[int(o): int(o) + (1 << n)] for o, n in zip(self.offsets, self.n_powers)]
+
+    def execute(self, a, b, out=None, stream=None):
+        import torch
+        if out is None:
+            out = torch.empty_like(a)
+        check(lib().gpufft_batch_plan_execute(self.h, _ptr(a), _ptr(b), _ptr(out), _stream_handle(stream)),
+              "batch_plan_execute")
+        return out
+
+    def autotune(self, a, b, out, cache_path=None, stream=None):
+        cp = cache_path.encode() if cache_path else None
+        check(lib().gpufft_batch_plan_autotune(self.h, _ptr(a), _ptr(b), _ptr(out), cp, _stream_handle(stream)),
+              "batch_plan_autotune")
+        return self.info()
+
+    def capture(self, a, b, out, stream):
+        check(lib().gpufft_batch_plan_capture(self.h, _ptr(a), _ptr(b), _ptr(out), _stream_handle(stream)),
+              "batch_plan_capture")
+
+    def replay(self, stream):
+        check(lib().gpufft_batch_plan_replay(self.h, _stream_handle(stream)), "batch_plan_replay")
+
+    def info(self):
+        m, g, gr, ws = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        check(lib().gpufft_batch_plan_info(self.h, ctypes.byref(m), ctypes.byref(g), ctypes.byref(gr),
+                                           ctypes.byref(ws)), "batch_plan_info")
+        return {"ctas_per_sm": m.value, "items_per_grab": g.value, "grid": gr.value, "workspace_bytes": ws.value}
+
+    def status(self):
+        f = ctypes.c_int()
+        check(lib().gpufft_batch_plan_status(self.h, ctypes.byref(f)), "batch_plan_status")
+        return f.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpufft_batch_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -71,6 +71,37 @@ namespace gfb
 int set_cuda_error(cudaError_t e);
 int check_launch();
 
+// Number of SMs of the current device (cached per device ordinal).
+inline int sm_count()
+{
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cache[dev])
+    {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+// Round a wave of `w` products down so that w * tiles_per_product CTAs fill
+// whole waves of the SMs, when that keeps at least one full step.
+inline long long round_wave(long long w, long long tiles_per_product)
+{
+    long long a = sm_count(), b = tiles_per_product;
+    while (b)
+    {
+        const long long t = a % b;
+        a = b;
+        b = t;
+    }
+    const long long step = sm_count() / a;
+    if (w >= step) w -= w % step;
+    return w;
+}
+
 // Opt a kernel into more than 48 KB of dynamic shared memory, once per device.
 // `done` must be a per-kernel array of 64 ints (one slot per device ordinal).
 template <typename K> int ensure_smem(K* kernel, size_t bytes, int* done)

@@ -1,0 +1,108 @@
+// gpufft-b200: the fused product pass (forward of both operands, pointwise
+// product, inverse) as a device function, shared by the product kernels and
+// the batched multi-size kernel.
+#pragma once
+
+#include "gf_pass.cuh"
+
+namespace gfb
+{
+
+template <typename T> struct FusedArgs
+{
+    const T* a;
+    const T* b;
+    T* c;
+    cx<T>* ws;
+    const cx<T>* roots;
+    const cx<T>* inv_roots;
+    const cx<T>* twist;
+    const cx<T>* untwist;
+    T scale;
+    long long batch; // products handled by this launch
+    PassGeo geo;
+    int lin; // linear (zero-padded) operands: rows of M reals, x_j = f_j
+};
+
+// Contiguous pass over both operands: all forward stages of the pass on A and
+// B, the pointwise product, and all inverse stages on the product. SINGLE: the
+// pass is the whole transform (fold + twist in the load, scale + untwist +
+// unfold in the store); otherwise A/B come from and the product returns to the
+// workspace.
+template <typename T, int L, bool SINGLE>
+__device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta, cx<T>* sm)
+{
+    using S = Sched<0, L>;
+    constexpr int W0 = S::win(0, true), WM = S::win(S::n - 1, true), WE = S::win(S::n - 1, false);
+    const int t = threadIdx.x;
+    const long long M = 1LL << a.geo.m;
+
+    cx<T> x[2][RPT];
+    TwCtx c;
+    {
+        const Tile<L, false, W0> tl(a.geo, cta, t);
+        c.g = tl.g;
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+        {
+            if (tl.b[r] < a.batch)
+            {
+                if (SINGLE)
+                {
+                    const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
+                    if (a.lin)
+                    {
+                        x[0][r] = cmul<T>(mk<T>(ld_stream(a.a + tl.b[r] * M + tl.j[r]), T(0)), tw);
+                        x[1][r] = cmul<T>(mk<T>(ld_stream(a.b + tl.b[r] * M + tl.j[r]), T(0)), tw);
+                    }
+                    else
+                    {
+                        const T* pa = a.a + tl.b[r] * 2 * M + tl.j[r];
+                        const T* pb = a.b + tl.b[r] * 2 * M + tl.j[r];
+                        x[0][r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
+                        x[1][r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
+                    }
+                }
+                else
+                {
+                    x[0][r] = a.ws[tl.b[r] * M + tl.j[r]];
+                    x[1][r] = a.ws[(a.batch + tl.b[r]) * M + tl.j[r]];
+                }
+            }
+            else
+            {
+                x[0][r] = mk<T>(T(0), T(0));
+                x[1][r] = x[0][r];
+            }
+        }
+    }
+    c.s0 = a.geo.s0;
+    c.neg = 0;
+
+    run_rounds<T, true, 0, L, 2>(x, sm, a.roots, c, t);
+    static_assert(WM == S::win(0, false), "the inverse starts where the forward ends");
+    cx<T> z[1][RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) z[0][r] = cmul<T>(x[0][r], x[1][r]);
+    run_rounds<T, false, 0, L, 1>(z, sm, a.inv_roots, c, t);
+
+    const Tile<L, false, WE> tl(a.geo, cta, t);
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+    {
+        if (tl.b[r] >= a.batch) continue;
+        if (SINGLE)
+        {
+            const cx<T> v = cmul<T>(cmul<T>(z[0][r], mk<T>(a.scale, T(0))), ldg<T>(a.untwist + tl.j[r]));
+            T* pc = a.c + tl.b[r] * 2 * M + tl.j[r];
+            st_stream(pc, v.x);
+            st_stream(pc + M, v.y);
+        }
+        else
+        {
+            a.ws[tl.b[r] * M + tl.j[r]] = z[0][r];
+        }
+    }
+}
+
+} // namespace gfb

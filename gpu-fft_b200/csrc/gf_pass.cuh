@@ -14,13 +14,22 @@ enum InKind
     IN_REAL = 1, // real promoted to complex (fft.cu:303-305)
     IN_FOLD = 2, // FFNT fold f_j + i f_{j+M} then twist (fft.cu:1057-1069)
     IN_PROD = 3, // product of the two complex operands (fft.cu:194-205, 1252-1263)
-    IN_FOLD2 = 4 // IN_FOLD with batch entries [0, split) from `in`, the rest from `in2`
+    IN_FOLD2 = 4, // IN_FOLD with batch entries [0, split) from `in`, the rest from `in2`
+    IN_LIN2 = 5,  // zero-padded linear operand: x_j = f_j (real, rows of M), then twist;
+                  // batch entries [0, split) from `in`, the rest from `in2`
+    IN_VJP3 = 6,  // batch entries [0, split): IN_FOLD from `in` (rows of 2M);
+                  // [split, 2 split): IN_LIN from `in2`; [2 split, 3 split): IN_LIN from `in3`
+    IN_GROUP = 7  // split product: transform b = s W + p is the limb group
+                  // C^_s = sum_{i+j=s} A^_i B^_j (+ centring term) of product p,
+                  // from the limb spectra [2k][W][M] at `in`
 };
 enum OutKind
 {
     OUT_CPX = 0,   // complex vector, optionally scaled by mod_inverse (fft.cu:246-253)
     OUT_REAL = 1,  // real part of the scaled value (fft.cu:499-514)
-    OUT_UNFOLD = 2 // scale, untwist, unfold re -> j, im -> j+M (fft.cu:1366-1383)
+    OUT_UNFOLD = 2, // scale, untwist, unfold re -> j, im -> j+M (fft.cu:1366-1383)
+    OUT_RE2 = 3     // scale, untwist, keep the real part (coefficient j < M) only;
+                    // batch entries [0, split) to `out`, the rest to `out2`
 };
 
 // Geometry of one pass (stages [s0, s0+L) of a 2^m transform); L and the
@@ -36,8 +45,10 @@ struct PassGeo
 template <typename T> struct PassArgs
 {
     const void* in;
-    const void* in2; // IN_FOLD2: second operand array
+    const void* in2; // IN_FOLD2 / IN_LIN2 / IN_VJP3: second operand array
+    const void* in3; // IN_VJP3: third operand array
     void* out;
+    void* out2;      // OUT_RE2: second output array
     const cx<T>* table;
     const cx<T>* twist;
     cx<T> scale;
@@ -48,6 +59,11 @@ template <typename T> struct PassArgs
     int in_kind, out_kind;
     int zero_pad; // forward first pass: the upper half of each input is zero
     int do_scale; // last inverse pass: multiply by scale
+    // IN_GROUP (split product)
+    long long W;          // products per wave
+    const cx<T>* uspec;   // transform of the all-ones polynomial
+    int gk, gcentre;      // limbs; centred inputs
+    int uq, ur;           // centring term joins group l + uq, scaled by 2^ur
 };
 
 // Where the 16 registers of thread t (window W) live: batch entry b[r] and
@@ -126,6 +142,51 @@ __device__ __forceinline__ cx<T> load_elem(const PassArgs<T>& a, int kind, long 
         const cx<T> f = mk<T>(ld_stream(p), ld_stream(p + M));
         return cmul<T>(f, ldg<T>(a.twist + j));
     }
+    else if (kind == IN_LIN2)
+    {
+        const T* base = reinterpret_cast<const T*>(a.in);
+        if (b >= a.split)
+        {
+            base = reinterpret_cast<const T*>(a.in2);
+            b -= a.split;
+        }
+        return cmul<T>(mk<T>(ld_stream(base + b * M + j), T(0)), ldg<T>(a.twist + j));
+    }
+    else if (kind == IN_VJP3)
+    {
+        if (b < a.split)
+        {
+            const T* p = reinterpret_cast<const T*>(a.in) + b * 2 * M + j;
+            return cmul<T>(mk<T>(ld_stream(p), ld_stream(p + M)), ldg<T>(a.twist + j));
+        }
+        const T* base = reinterpret_cast<const T*>(b < 2 * a.split ? a.in2 : a.in3);
+        b -= (b < 2 * a.split) ? a.split : 2 * a.split;
+        return cmul<T>(mk<T>(ld_stream(base + b * M + j), T(0)), ldg<T>(a.twist + j));
+    }
+    else if (kind == IN_GROUP)
+    {
+        const long long sg = b / a.W, p = b - sg * a.W;
+        const cx<T>* sp = reinterpret_cast<const cx<T>*>(a.in) + p * M + j;
+        const long long st = a.W * M; // stride between limb spectra
+        const int k = a.gk;
+        const int i0 = (int)sg - (k - 1) > 0 ? (int)sg - (k - 1) : 0;
+        cx<T> acc = mk<T>(T(0), T(0));
+        constexpr int KMAX = 8;
+#pragma unroll
+        for (int ii = 0; ii < KMAX; ii++)
+        {
+            const int i = i0 + ii;
+            if (i <= (int)sg && i < k) acc = cadd<T>(acc, cmul<T>(sp[i * st], sp[(k + sg - i) * st]));
+        }
+        const int l = (int)sg - a.uq;
+        if (a.gcentre && l >= 0 && l < k)
+        {
+            const cx<T> e = cadd<T>(sp[l * st], sp[(k + l) * st]);
+            const T sc = (T)(1 << a.ur);
+            acc = cadd<T>(acc, cmul<T>(mk<T>(e.x * sc, e.y * sc), ldg<T>(a.uspec + j)));
+        }
+        return acc;
+    }
     else
     {
         const cx<T>* p = reinterpret_cast<const cx<T>*>(a.in) + b * M + j;
@@ -147,12 +208,155 @@ __device__ __forceinline__ void store_elem(const PassArgs<T>& a, int kind, long 
         if (a.do_scale) v = cmul<T>(v, a.scale);
         reinterpret_cast<T*>(a.out)[b * M + j] = v.x;
     }
-    else
+    else if (kind == OUT_UNFOLD)
     {
         v = cmul<T>(cmul<T>(v, a.scale), ldg<T>(a.twist + j));
         T* p = reinterpret_cast<T*>(a.out) + b * 2 * M + j;
         p[0] = v.x;
         p[M] = v.y;
+    }
+    else
+    {
+        v = cmul<T>(cmul<T>(v, a.scale), ldg<T>(a.twist + j));
+        T* base = reinterpret_cast<T*>(b < a.split ? a.out : a.out2);
+        b -= (b < a.split) ? 0 : a.split;
+        st_stream(base + b * M + j, v.x);
+    }
+}
+
+// Row pointers of one batch entry for the load kinds whose rows are real
+// coefficients (fold pairs f_j, f_{j+M}, or linear rows with zero imaginary
+// part): selected once per CTA when the whole tile lies in one batch entry.
+template <typename T> struct RealRows
+{
+    const T* re;
+    long long im_off; // offset of f_{j+M} from f_j; < 0: imaginary part is zero
+};
+
+template <typename T>
+__device__ __forceinline__ RealRows<T> real_rows(const PassArgs<T>& a, int kind, long long b)
+{
+    const long long M = 1LL << a.geo.m;
+    RealRows<T> r;
+    if (kind == IN_FOLD || kind == IN_FOLD2)
+    {
+        const T* base = reinterpret_cast<const T*>((kind == IN_FOLD2 && b >= a.split) ? a.in2 : a.in);
+        if (kind == IN_FOLD2 && b >= a.split) b -= a.split;
+        r.re = base + b * 2 * M;
+        r.im_off = M;
+    }
+    else if (kind == IN_LIN2)
+    {
+        const T* base = reinterpret_cast<const T*>(b >= a.split ? a.in2 : a.in);
+        if (b >= a.split) b -= a.split;
+        r.re = base + b * M;
+        r.im_off = -1;
+    }
+    else // IN_VJP3
+    {
+        if (b < a.split)
+        {
+            r.re = reinterpret_cast<const T*>(a.in) + b * 2 * M;
+            r.im_off = M;
+        }
+        else
+        {
+            const T* base = reinterpret_cast<const T*>(b < 2 * a.split ? a.in2 : a.in3);
+            b -= (b < 2 * a.split) ? a.split : 2 * a.split;
+            r.re = base + b * M;
+            r.im_off = -1;
+        }
+    }
+    return r;
+}
+
+// One pass of CTA-tile `cta` (sm: SMEM_ELEMS complex elements of shared memory).
+template <typename T, bool FWD, int L, bool STRIDED>
+__device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, cx<T>* sm)
+{
+    constexpr int QOFF = STRIDED ? EBITS - L : 0;
+    using S = Sched<QOFF, L>;
+    constexpr int W0 = S::win(0, FWD), WL = S::win(S::n - 1, FWD);
+    const int t = threadIdx.x;
+    // the tile lies in one batch entry: strided passes, and contiguous passes of
+    // transforms with at least ECTA elements
+    const bool one_entry = STRIDED || a.geo.m >= EBITS;
+
+    cx<T> x[1][RPT];
+    TwCtx c;
+    {
+        const Tile<L, STRIDED, W0> tl(a.geo, cta, t);
+        c.g = tl.g;
+        const int kind = a.in_kind;
+        const bool real_rows_kind = kind == IN_FOLD || kind == IN_FOLD2 || kind == IN_LIN2 || kind == IN_VJP3;
+        if (one_entry && real_rows_kind && tl.b[0] < a.batch)
+        {
+            // straight-line loads: every address is row + j
+            const RealRows<T> rr = real_rows<T>(a, kind, tl.b[0]);
+            T re[RPT], im[RPT];
+            cx<T> tw[RPT];
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+            {
+                re[r] = ld_stream(rr.re + tl.j[r]);
+                im[r] = (rr.im_off >= 0) ? ld_stream(rr.re + rr.im_off + tl.j[r]) : T(0);
+                tw[r] = ldg<T>(a.twist + tl.j[r]);
+            }
+#pragma unroll
+            for (int r = 0; r < RPT; r++) x[0][r] = cmul<T>(mk<T>(re[r], im[r]), tw[r]);
+        }
+        else if (one_entry && kind == IN_CPX && tl.b[0] < a.batch)
+        {
+            const long long M = 1LL << a.geo.m;
+            const cx<T>* row = reinterpret_cast<const cx<T>*>(a.in) + tl.b[0] * M;
+            const bool zp = a.zero_pad != 0;
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                x[0][r] = (zp && tl.j[r] >= (M >> 1)) ? mk<T>(T(0), T(0)) : row[tl.j[r]];
+        }
+        else
+        {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                x[0][r] = (tl.b[r] < a.batch) ? load_elem<T>(a, kind, tl.b[r], tl.j[r]) : mk<T>(T(0), T(0));
+        }
+    }
+    c.s0 = a.geo.s0;
+    c.neg = a.geo.neg;
+    run_rounds<T, FWD, QOFF, L, 1>(x, sm, a.table, c, t);
+    {
+        const Tile<L, STRIDED, WL> tl(a.geo, cta, t);
+        const int kind = a.out_kind;
+        if (one_entry && tl.b[0] < a.batch && (kind == OUT_UNFOLD || kind == OUT_CPX))
+        {
+            const long long M = 1LL << a.geo.m;
+            if (kind == OUT_UNFOLD)
+            {
+                T* row = reinterpret_cast<T*>(a.out) + tl.b[0] * 2 * M;
+                cx<T> u[RPT];
+#pragma unroll
+                for (int r = 0; r < RPT; r++) u[r] = ldg<T>(a.twist + tl.j[r]);
+#pragma unroll
+                for (int r = 0; r < RPT; r++)
+                {
+                    const cx<T> v = cmul<T>(cmul<T>(x[0][r], a.scale), u[r]);
+                    st_stream(row + tl.j[r], v.x);
+                    st_stream(row + M + tl.j[r], v.y);
+                }
+            }
+            else
+            {
+                cx<T>* row = reinterpret_cast<cx<T>*>(a.out) + tl.b[0] * M;
+#pragma unroll
+                for (int r = 0; r < RPT; r++) row[tl.j[r]] = a.do_scale ? cmul<T>(x[0][r], a.scale) : x[0][r];
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                if (tl.b[r] < a.batch) store_elem<T>(a, kind, tl.b[r], tl.j[r], x[0][r]);
+        }
     }
 }
 
@@ -160,33 +364,7 @@ template <typename T, bool FWD, int L, bool STRIDED>
 __global__ void __launch_bounds__(NTHR, 2) pass_kernel(const PassArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-    constexpr int QOFF = STRIDED ? EBITS - L : 0;
-    using S = Sched<QOFF, L>;
-    constexpr int W0 = S::win(0, FWD), WL = S::win(S::n - 1, FWD);
-    const int t = threadIdx.x;
-    const long long cta = blockIdx.x;
-
-    cx<T> x[1][RPT];
-    {
-        const Tile<L, STRIDED, W0> tl(a.geo, cta, t);
-        const int kind = a.in_kind;
-#pragma unroll
-        for (int r = 0; r < RPT; r++)
-            x[0][r] = (tl.b[r] < a.batch) ? load_elem<T>(a, kind, tl.b[r], tl.j[r]) : mk<T>(T(0), T(0));
-    }
-    TwCtx c;
-    c.g = Tile<L, STRIDED, W0>(a.geo, cta, t).g;
-    c.s0 = a.geo.s0;
-    c.neg = a.geo.neg;
-    run_rounds<T, FWD, QOFF, L, 1>(x, sm, a.table, c, t);
-    {
-        const Tile<L, STRIDED, WL> tl(a.geo, cta, t);
-        const int kind = a.out_kind;
-#pragma unroll
-        for (int r = 0; r < RPT; r++)
-            if (tl.b[r] < a.batch) store_elem<T>(a, kind, tl.b[r], tl.j[r], x[0][r]);
-    }
+    pass_body<T, FWD, L, STRIDED>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
 }
 
 // ---------------------------------------------------------------------------

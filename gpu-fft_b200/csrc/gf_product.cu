@@ -19,16 +19,21 @@
 //
 // Twiddles come from gpufft_ffnt_make_tables_*, generated on the device with
 // sincospi in double precision (then rounded to float for the f32 path).
-#include "gf_pass.cuh"
+#include "gf_fused.cuh"
 
 namespace gfb
 {
 
 // ---------------------------------------------------------------------------
-// device twiddle tables:  [roots M/2 | inverse roots M/2 | twist M | untwist M]
+// device twiddle tables:  [roots M/2 | inverse roots M/2 | twist M | untwist M | U M]
 // roots[i] = e^{+2 pi i bitrev_{m-1}(i) / M}, twist[j] = e^{+i pi j / N}, M = N/2
 // (the values of the reference's ReverseRootTable_ffnt / twist_table_ffnt,
 // fft_cpu.cu:251-297, 435-473, computed here in double precision).
+// U[r] is the FFNT spectrum of the all-ones polynomial u = 1 + X + ... + X^(N-1)
+// in the transform's output order: at frequency k = bitrev_m(r),
+//     U = sum_j (1+i) psi^j w^(jk) = 2 / (1 - e^{i theta}) = 1 + i cot(theta/2),
+// theta = pi (4k+1) / (2M). The split-precision product uses it to centre its
+// inputs without an integer prefix scan.
 // ---------------------------------------------------------------------------
 template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
 {
@@ -49,98 +54,18 @@ template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
         sincospi((double)i / (double)(2 * M), &s, &c);
         tab[2 * H + i] = mk<T>((T)c, (T)s);
         tab[2 * H + M + i] = mk<T>((T)c, (T)-s);
+        const unsigned k = (m > 0) ? (__brev((unsigned)i) >> (32 - m)) : 0u;
+        double sh, ch;
+        sincospi((4.0 * (double)k + 1.0) / (4.0 * (double)M), &sh, &ch);
+        tab[2 * H + 2 * M + i] = mk<T>((T)1, (T)(ch / sh));
     }
 }
 
-template <typename T> struct FusedArgs
-{
-    const T* a;
-    const T* b;
-    T* c;
-    cx<T>* ws;
-    const cx<T>* roots;
-    const cx<T>* inv_roots;
-    const cx<T>* twist;
-    const cx<T>* untwist;
-    T scale;
-    long long batch; // products handled by this launch
-    PassGeo geo;
-};
-
-// Contiguous pass over both operands: all forward stages of the pass on A and
-// B, the pointwise product, and all inverse stages on the product. SINGLE: the
-// pass is the whole transform (fold + twist in the load, scale + untwist +
-// unfold in the store); otherwise A/B come from and the product returns to the
-// workspace.
 template <typename T, int L, bool SINGLE>
 __global__ void __launch_bounds__(NTHR, 1) fused_kernel(const FusedArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-    using S = Sched<0, L>;
-    constexpr int W0 = S::win(0, true), WM = S::win(S::n - 1, true), WE = S::win(S::n - 1, false);
-    const int t = threadIdx.x;
-    const long long cta = blockIdx.x;
-    const long long M = 1LL << a.geo.m;
-
-    cx<T> x[2][RPT];
-    TwCtx c;
-    {
-        const Tile<L, false, W0> tl(a.geo, cta, t);
-        c.g = tl.g;
-#pragma unroll
-        for (int r = 0; r < RPT; r++)
-        {
-            if (tl.b[r] < a.batch)
-            {
-                if (SINGLE)
-                {
-                    const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
-                    const T* pa = a.a + tl.b[r] * 2 * M + tl.j[r];
-                    const T* pb = a.b + tl.b[r] * 2 * M + tl.j[r];
-                    x[0][r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
-                    x[1][r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
-                }
-                else
-                {
-                    x[0][r] = a.ws[tl.b[r] * M + tl.j[r]];
-                    x[1][r] = a.ws[(a.batch + tl.b[r]) * M + tl.j[r]];
-                }
-            }
-            else
-            {
-                x[0][r] = mk<T>(T(0), T(0));
-                x[1][r] = x[0][r];
-            }
-        }
-    }
-    c.s0 = a.geo.s0;
-    c.neg = 0;
-
-    run_rounds<T, true, 0, L, 2>(x, sm, a.roots, c, t);
-    static_assert(WM == S::win(0, false), "the inverse starts where the forward ends");
-    cx<T> z[1][RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; r++) z[0][r] = cmul<T>(x[0][r], x[1][r]);
-    run_rounds<T, false, 0, L, 1>(z, sm, a.inv_roots, c, t);
-
-    const Tile<L, false, WE> tl(a.geo, cta, t);
-#pragma unroll
-    for (int r = 0; r < RPT; r++)
-    {
-        if (tl.b[r] >= a.batch) continue;
-        if (SINGLE)
-        {
-            const cx<T> v = cmul<T>(cmul<T>(z[0][r], mk<T>(a.scale, T(0))), ldg<T>(a.untwist + tl.j[r]));
-            T* pc = a.c + tl.b[r] * 2 * M + tl.j[r];
-            st_stream(pc, v.x);
-            st_stream(pc + M, v.y);
-        }
-        else
-        {
-            a.ws[tl.b[r] * M + tl.j[r]] = z[0][r];
-        }
-    }
+    fused_body<T, L, SINGLE>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
 }
 
 template <typename T, int L, bool SINGLE>
@@ -173,12 +98,16 @@ static long long wave_products(int n_power, long long batch, size_t cx_bytes)
     const size_t per = 2 * ((size_t)1 << m) * cx_bytes;
     long long w = (long long)(WAVE_TARGET_BYTES / per);
     if (w < 1) w = 1;
+    w = round_wave(w, ((long long)1 << m) / ECTA);
     return w < batch ? w : batch;
 }
 
+// lin = 0: c = a b mod (X^N + 1), N = 2^n_power, a/b/c rows of N.
+// lin = 1: the linear product of rows of N/2 (a, b zero-padded to N; the
+//          product has degree < N - 1 so no wrap-around), c rows of N.
 template <typename T>
 static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, const void* tables, void* ws,
-                          size_t ws_bytes, cudaStream_t s)
+                          size_t ws_bytes, cudaStream_t s, int lin = 0)
 {
     if (n_power < NATIVE_MIN_NPOWER || n_power > NATIVE_MAX_NPOWER) return GPUFFT_ERROR_INVALID_N_POWER;
     if (!a || !b || !c || !tables || batch <= 0) return GPUFFT_ERROR_INVALID_VALUE;
@@ -194,6 +123,8 @@ static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, 
     f.twist = tab + M;
     f.untwist = tab + 2 * M;
     f.scale = (T)(1.0 / (double)M);
+    f.lin = lin;
+    const long long in_row = lin ? M : 2 * M; // reals per input row
 
     if (m <= EBITS)
     {
@@ -221,14 +152,14 @@ static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, 
             long long ctas = 0;
             PassArgs<T> k{};
             k.geo = pass_geo(p, 0, m, 0, 2 * w, &ctas);
-            k.in = a + p0 * 2 * M;
-            k.in2 = b + p0 * 2 * M;
+            k.in = a + p0 * in_row;
+            k.in2 = b + p0 * in_row;
             k.split = w;
             k.out = wsp;
             k.table = f.roots;
             k.twist = f.twist;
             k.batch = 2 * w;
-            k.in_kind = IN_FOLD2;
+            k.in_kind = lin ? IN_LIN2 : IN_FOLD2;
             k.out_kind = OUT_CPX;
             int st = launch_pass<T, true>(k, p, 0, ctas, s);
             if (st) return st;
@@ -281,8 +212,8 @@ template <typename T> static int make_tables(int n_power, void* tables, cudaStre
 extern "C" size_t gpufft_ffnt_tables_count(int n_power)
 {
     if (n_power < gfb::NATIVE_MIN_NPOWER || n_power > 25) return 0;
-    // [roots M/2 | inverse roots M/2 | twist M | untwist M], M = N/2
-    return (size_t)3 << (n_power - 1);
+    // [roots M/2 | inverse roots M/2 | twist M | untwist M | U M], M = N/2
+    return (size_t)4 << (n_power - 1);
 }
 
 extern "C" int gpufft_ffnt_make_tables_f32(int n_power, void* tables, gpufft_stream_t stream)
@@ -385,4 +316,33 @@ extern "C" int gpufft_negacyclic_mul_f64_noalloc(const double* a, const double* 
     if (st) return st;
     return gfb::negacyclic_mul<double>(a, b, c, n_power, batch, tables, scratch, gfb::NOALLOC_SCRATCH_BYTES,
                                        (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Linear product of real polynomials (the R_R product of the reference,
+// reference fft.cu:600-725 with example/test_fft_gpu_R_R.cu's zero padding):
+// computed as the negacyclic product of length 2N whose upper input halves are
+// zero, so each operand folds into N real complex values -- a half-length
+// transform, where the reference transforms 2N complex values.
+// ---------------------------------------------------------------------------
+extern "C" size_t gpufft_linear_mul_workspace_bytes(int n_power, int batch, int precision_bits)
+{
+    return gpufft_negacyclic_mul_workspace_bytes(n_power + 1, batch, precision_bits);
+}
+
+extern "C" int gpufft_linear_mul_f32(const float* a, const float* b, float* c, int n_power, int batch,
+                                     const void* tables, void* workspace, size_t workspace_bytes,
+                                     gpufft_stream_t stream)
+{
+    if (n_power < 1 || n_power > gfb::NATIVE_MAX_NPOWER - 1) return GPUFFT_ERROR_INVALID_N_POWER;
+    return gfb::negacyclic_mul<float>(a, b, c, n_power + 1, batch, tables, workspace, workspace_bytes,
+                                      (cudaStream_t)stream, 1);
+}
+extern "C" int gpufft_linear_mul_f64(const double* a, const double* b, double* c, int n_power, int batch,
+                                     const void* tables, void* workspace, size_t workspace_bytes,
+                                     gpufft_stream_t stream)
+{
+    if (n_power < 1 || n_power > gfb::NATIVE_MAX_NPOWER - 1) return GPUFFT_ERROR_INVALID_N_POWER;
+    return gfb::negacyclic_mul<double>(a, b, c, n_power + 1, batch, tables, workspace, workspace_bytes,
+                                       (cudaStream_t)stream, 1);
 }

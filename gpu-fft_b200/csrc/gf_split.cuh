@@ -1,0 +1,438 @@
+// gpufft-b200: FP32 split-precision negacyclic product with exact int64 output.
+//
+// c = a * b mod (X^N + 1) for integer coefficients, computed exactly with
+// single-precision transforms:
+//   1. every coefficient is cut into k balanced signed digits of w bits,
+//      x = sum_l d_l 2^(w l), d_l in [-2^(w-1), 2^(w-1)) (the top digit takes
+//      what is left), giving k small-integer "limb" polynomials per operand;
+//   2. each limb polynomial goes through the FFNT forward transform (fold,
+//      twist, half-length FFT; reference fft.cu:1013-1212) in FP32;
+//   3. for every shift s = 0 .. 2k-2 the limb spectra are combined pointwise,
+//      C^_s = sum_{i+j=s} A^_i B^_j, and C_s is brought back by the inverse
+//      transform (reference fft.cu:1214-1384);
+//   4. each C_s is rounded to an integer and c = sum_s C_s 2^(w s) is formed in
+//      exact int64 arithmetic (wrapping modulo 2^64).
+// The limb width is chosen so that every C_s stays well inside FP32's exact
+// range (an error model calibrated on this transform); the largest distance
+// of any C_s value to its nearest integer ("pre-rounding error") is measured
+// on the device and returned, so exactness (error < 0.5) is checked per call.
+//
+// Kernels (N > 8192, per wave of products; workspace in L2):
+//   split_fwd0   strided first forward pass for the 2k limb polynomials of a
+//                product column block: the int32 inputs are loaded once, each
+//                limb is extracted, folded, twisted and transformed in turn;
+//   split_mid    contiguous last forward pass of all 2k limb spectra, the
+//                2k-1 pointwise group sums and the first inverse pass of each;
+//   split_inv0   strided last inverse pass of every group with scale, untwist,
+//                unfold, rounding and the int64 recombination in registers.
+// N <= 8192 runs all of it in one kernel (split_mid<true>).
+#pragma once
+
+#include "gf_pass.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace gfb
+{
+
+constexpr int SPLIT_MAX_LIMBS = 8;
+
+// Balanced signed digit l (width w, k digits) of v.
+__device__ __forceinline__ int limb_digit(long long v, int l, int w, int k)
+{
+    const long long base = 1LL << w, half = base >> 1;
+    long long d = 0;
+    for (int i = 0; i <= l; i++)
+    {
+        if (i == k - 1)
+        {
+            d = v;
+        }
+        else
+        {
+            const long long r = v & (base - 1);
+            d = (r >= half) ? r - base : r;
+        }
+        v = (v - d) >> w;
+    }
+    return (int)d;
+}
+
+struct SplitArgs
+{
+    const int32_t* a;
+    const int32_t* b;
+    int64_t* c;
+    cx<float>* spec;  // [2k][W][M] limb spectra (operand-major: a limbs then b limbs)
+    cx<float>* group; // [2k-1][W][M] group spectra
+    const cx<float>* roots;
+    const cx<float>* inv_roots;
+    const cx<float>* twist;
+    const cx<float>* untwist;
+    unsigned* max_err; // float bits of the largest pre-rounding error (may be null)
+    const cx<float>* uspec; // transform of the all-ones polynomial (table block)
+    long long K;       // centring offset subtracted from every coefficient (0: none)
+    int uq, ur;        // K = 2^(w uq + ur): centring term joins groups s = l + uq, scaled 2^ur
+    float scale;
+    int w, k;
+    long long W; // products per wave (stride of the workspace)
+    long long batch;
+    PassGeo geo;
+};
+
+// Distance of a group value to its nearest integer. Above 2^22 every float is
+// (nearly) an integer and the distance no longer certifies exactness, so such
+// values report 1.0.
+__device__ __forceinline__ float group_error(cx<float> v, float rr, float ri)
+{
+    const float lim = 4194304.0f; // 2^22
+    if (fabsf(v.x) >= lim || fabsf(v.y) >= lim) return 1.0f;
+    return fmaxf(fabsf(v.x - rr), fabsf(v.y - ri));
+}
+
+__device__ __forceinline__ void report_err(unsigned* dst, float e)
+{
+    if (!dst) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(dst, __float_as_uint(e));
+}
+
+// Non-negative inputs are centred before they are cut into limbs,
+// a = a' + K u with u = 1 + X + ... + X^(N-1) and K = 2^(B) (B = input_bits-1),
+// so that every limb is balanced (a non-centred top limb would make its group
+// values grow like N * mean^2). The product is then
+//     a b = a'b' + K (a' u + b' u) + K^2 u u        (mod X^N + 1).
+// With K = 2^(w q + r) (0 <= r < w) the middle term is
+//     sum_l 2^(w (l + q)) * 2^r (e^a_l + e^b_l) u,
+// i.e. 2^r (E^a_l + E^b_l) U joins limb group s = l + q in the frequency domain
+// (U = transform of u, part of the native table block), and K^2 u u, whose
+// coefficients are K^2 (2k + 2 - N), is added exactly in int64 at the end.
+__device__ __forceinline__ long long uu_term(const SplitArgs& a, long long k, long long N)
+{
+    return (long long)((unsigned long long)a.K * (unsigned long long)a.K * (unsigned long long)(2 * k + 2 - N));
+}
+
+// --------------------------------------------------------------------------
+// strided first forward pass of every limb polynomial
+// --------------------------------------------------------------------------
+template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const SplitArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
+    constexpr int QOFF = EBITS - L;
+    using S = Sched<QOFF, L>;
+    constexpr int W0 = S::win(0, true), WL = S::win(S::n - 1, true);
+    const int t = threadIdx.x;
+    const long long cta = blockIdx.x;
+    const long long M = 1LL << a.geo.m;
+
+    // the raw coefficients (fold pair j, j+M) of this CTA's elements, loaded once
+    const Tile<L, true, W0> tl(a.geo, cta, t); // batch index = operand * W + product
+    const long long op = tl.b[0] / a.W, p = tl.b[0] - op * a.W;
+    const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M;
+    int vlo[RPT], vhi[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+    {
+        vlo[r] = (int)((long long)__ldcs(src + tl.j[r]) - a.K);
+        vhi[r] = (int)((long long)__ldcs(src + tl.j[r] + M) - a.K);
+    }
+    TwCtx c;
+    c.g = tl.g;
+    c.s0 = 0;
+    c.neg = 0;
+    const Tile<L, true, WL> to(a.geo, cta, t);
+    for (int l = 0; l < a.k; l++)
+    {
+        cx<float> x[1][RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+        {
+            const cx<float> f = mk<float>((float)limb_digit(vlo[r], l, a.w, a.k), (float)limb_digit(vhi[r], l, a.w, a.k));
+            x[0][r] = cmul<float>(f, ldg<float>(a.twist + tl.j[r]));
+        }
+        if (l > 0) __syncthreads();
+        run_rounds<float, true, QOFF, L, 1>(x, sm, a.roots, c, t);
+        cx<float>* dst = a.spec + ((op * a.k + l) * a.W + p) * M;
+#pragma unroll
+        for (int r = 0; r < RPT; r++) dst[to.j[r]] = x[0][r];
+    }
+}
+
+// --------------------------------------------------------------------------
+// contiguous middle: last forward pass of the 2k limb spectra, group sums,
+// first inverse pass of every group (SINGLE: whole transforms, int32 in,
+// int64 out, everything in this kernel)
+// --------------------------------------------------------------------------
+template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) split_mid(const SplitArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
+    using S = Sched<0, L>;
+    constexpr int W0 = S::win(0, true), WM = S::win(S::n - 1, true), WE = S::win(S::n - 1, false);
+    constexpr int NG = 2 * K - 1;
+    const int t = threadIdx.x;
+    const long long cta = blockIdx.x;
+    const long long M = 1LL << a.geo.m;
+
+    const Tile<L, false, W0> ti(a.geo, cta, t);
+    const Tile<L, false, WM> tm(a.geo, cta, t);
+    TwCtx c;
+    c.g = ti.g;
+    c.s0 = a.geo.s0;
+    c.neg = 0;
+
+    // 1. last forward pass (SINGLE: every forward stage, limb extraction in the
+    //    load) of every limb spectrum; results parked in a.spec
+    for (int tau = 0; tau < 2 * K; tau++)
+    {
+        const int op = tau / K, l = tau - op * K;
+        cx<float> x[1][RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+        {
+            if (ti.b[r] >= a.batch)
+            {
+                x[0][r] = mk<float>(0.f, 0.f);
+                continue;
+            }
+            if (SINGLE)
+            {
+                const int32_t* src = (op == 0 ? a.a : a.b) + ti.b[r] * 2 * M + ti.j[r];
+                const long long v0 = (long long)__ldg(src) - a.K, v1 = (long long)__ldg(src + M) - a.K;
+                const cx<float> f = mk<float>((float)limb_digit(v0, l, a.w, K), (float)limb_digit(v1, l, a.w, K));
+                x[0][r] = cmul<float>(f, ldg<float>(a.twist + ti.j[r]));
+            }
+            else
+            {
+                x[0][r] = a.spec[((long long)tau * a.W + ti.b[r]) * M + ti.j[r]];
+            }
+        }
+        if (tau > 0) __syncthreads();
+        run_rounds<float, true, 0, L, 1>(x, sm, a.roots, c, t);
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            if (tm.b[r] < a.batch) a.spec[((long long)tau * a.W + tm.b[r]) * M + tm.j[r]] = x[0][r];
+    }
+
+    // 2. group sums C^_s = sum_{i+j=s} A^_i B^_j (+ the centring term), four
+    //    elements at a time so that all 2K limb loads of a chunk are in flight
+    //    together; the thread reads only what it wrote in step 1
+    const float uscale = (float)(1 << a.ur);
+#pragma unroll
+    for (int ch = 0; ch < RPT / 4; ch++)
+    {
+        cx<float> v[2 * K][4], u[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+            const int r = 4 * ch + q;
+            const bool ok = tm.b[r] < a.batch;
+#pragma unroll
+            for (int tau = 0; tau < 2 * K; tau++)
+                v[tau][q] = ok ? a.spec[((long long)tau * a.W + tm.b[r]) * M + tm.j[r]] : mk<float>(0.f, 0.f);
+            u[q] = (a.K && ok) ? ldg<float>(a.uspec + tm.j[r]) : mk<float>(0.f, 0.f);
+        }
+#pragma unroll
+        for (int sg = 0; sg < NG; sg++)
+        {
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+            {
+                const int r = 4 * ch + q;
+                cx<float> acc = mk<float>(0.f, 0.f);
+#pragma unroll
+                for (int i = 0; i < K; i++)
+                    if (sg - i >= 0 && sg - i < K) acc = cadd<float>(acc, cmul<float>(v[i][q], v[K + sg - i][q]));
+                const int l = sg - a.uq;
+                if (a.K && l >= 0 && l < K)
+                {
+#pragma unroll
+                    for (int ll = 0; ll < K; ll++)
+                        if (ll == l)
+                        {
+                            const cx<float> e = cadd<float>(v[ll][q], v[K + ll][q]);
+                            acc = cadd<float>(acc, cmul<float>(mk<float>(e.x * uscale, e.y * uscale), u[q]));
+                        }
+                }
+                if (tm.b[r] < a.batch) a.group[((long long)sg * a.W + tm.b[r]) * M + tm.j[r]] = acc;
+            }
+        }
+    }
+
+    // 3. first inverse pass of every group (the whole inverse when SINGLE)
+    static_assert(WM == S::win(0, false), "the inverse starts where the forward ends");
+    long long acc_lo[RPT], acc_hi[RPT];
+    float err = 0.f;
+#pragma unroll
+    for (int r = 0; r < RPT; r++) acc_lo[r] = acc_hi[r] = 0;
+    const Tile<L, false, WE> te(a.geo, cta, t);
+    for (int sg = 0; sg < NG; sg++)
+    {
+        cx<float> x[1][RPT];
+        cx<float>* grp = a.group + (long long)sg * a.W * M;
+#pragma unroll
+        for (int r = 0; r < RPT; r++) x[0][r] = (tm.b[r] < a.batch) ? grp[tm.b[r] * M + tm.j[r]] : mk<float>(0.f, 0.f);
+        __syncthreads();
+        run_rounds<float, false, 0, L, 1>(x, sm, a.inv_roots, c, t);
+        if (SINGLE)
+        {
+            const int sh = a.w * sg;
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+            {
+                if (te.b[r] >= a.batch) continue;
+                const cx<float> v =
+                    cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j[r]));
+                const float rr = rintf(v.x), ri = rintf(v.y);
+                err = fmaxf(err, group_error(v, rr, ri));
+                acc_lo[r] += (long long)((unsigned long long)(long long)rr << sh);
+                acc_hi[r] += (long long)((unsigned long long)(long long)ri << sh);
+            }
+        }
+        else
+        {
+            // every thread has loaded its group-sg elements before any store:
+            // the rounds of an L = 12 pass contain block-wide barriers
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                if (te.b[r] < a.batch) grp[te.b[r] * M + te.j[r]] = x[0][r];
+        }
+    }
+    if (SINGLE)
+    {
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+        {
+            if (te.b[r] >= a.batch) continue;
+            int64_t* dst = a.c + te.b[r] * 2 * M + te.j[r];
+            __stcs(reinterpret_cast<long long*>(dst), acc_lo[r] + uu_term(a, te.j[r], 2 * M));
+            __stcs(reinterpret_cast<long long*>(dst + M), acc_hi[r] + uu_term(a, te.j[r] + M, 2 * M));
+        }
+        report_err(a.max_err, err);
+    }
+}
+
+// --------------------------------------------------------------------------
+// strided last inverse pass of every group, rounding and int64 recombination
+// --------------------------------------------------------------------------
+template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
+    constexpr int QOFF = EBITS - L;
+    using S = Sched<QOFF, L>;
+    constexpr int W0 = S::win(0, false), WE = S::win(S::n - 1, false);
+    const int t = threadIdx.x;
+    const long long cta = blockIdx.x;
+    const long long M = 1LL << a.geo.m;
+
+    const Tile<L, true, W0> ti(a.geo, cta, t); // batch index = product
+    const Tile<L, true, WE> te(a.geo, cta, t);
+    TwCtx c;
+    c.g = ti.g;
+    c.s0 = 0;
+    c.neg = 0;
+    const long long p = ti.b[0];
+
+    long long acc_lo[RPT], acc_hi[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) acc_lo[r] = acc_hi[r] = 0;
+    float err = 0.f;
+    for (int s = 0; s <= 2 * (a.k - 1); s++)
+    {
+        const cx<float>* src = a.group + ((long long)s * a.W + p) * M;
+        cx<float> x[1][RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++) x[0][r] = src[ti.j[r]];
+        if (s > 0) __syncthreads();
+        run_rounds<float, false, QOFF, L, 1>(x, sm, a.inv_roots, c, t);
+        const int sh = a.w * s;
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+        {
+            const cx<float> v =
+                cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j[r]));
+            const float rr = rintf(v.x), ri = rintf(v.y);
+            err = fmaxf(err, group_error(v, rr, ri));
+            acc_lo[r] += (long long)((unsigned long long)(long long)rr << sh);
+            acc_hi[r] += (long long)((unsigned long long)(long long)ri << sh);
+        }
+    }
+    int64_t* dst = a.c + p * 2 * M;
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+    {
+        __stcs(reinterpret_cast<long long*>(dst + te.j[r]), acc_lo[r] + uu_term(a, te.j[r], 2 * M));
+        __stcs(reinterpret_cast<long long*>(dst + te.j[r] + M), acc_hi[r] + uu_term(a, te.j[r] + M, 2 * M));
+    }
+    report_err(a.max_err, err);
+}
+
+constexpr int SPLIT_SINGLE_MAX_LIMBS = 6; // limb counts compiled for rings N <= 8192
+
+// Limb-group sums of a wave (rings N > 8192), one spectral point per thread:
+//     G_s[p][j] = sum_{i+l=s} A_i[p][j] B_l[p][j]  (+ 2^ur (A_l + B_l) U[j] for s = l + uq)
+// from the limb spectra [2K][W][M] into the group spectra [2K-1][W][M]. All 2K
+// loads of a point are independent and coalesced across the warp.
+template <int K> __global__ void __launch_bounds__(256) split_groups(const SplitArgs a)
+{
+    const long long M = 1LL << a.geo.m;
+    const long long n = a.W * M;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const long long j = idx & (M - 1);
+    cx<float> v[2 * K];
+#pragma unroll
+    for (int t = 0; t < 2 * K; t++) v[t] = __ldcs(a.spec + t * n + idx);
+    cx<float> u = mk<float>(0.f, 0.f);
+    if (a.K) u = ldg<float>(a.uspec + j);
+    const float uscale = (float)(1 << a.ur);
+#pragma unroll
+    for (int s = 0; s < 2 * K - 1; s++)
+    {
+        cx<float> acc = mk<float>(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < K; i++)
+            if (s - i >= 0 && s - i < K) acc = cadd<float>(acc, cmul<float>(v[i], v[K + s - i]));
+        if (a.K)
+        {
+#pragma unroll
+            for (int l = 0; l < K; l++)
+                if (l + a.uq == s)
+                {
+                    const cx<float> e = cadd<float>(v[l], v[K + l]);
+                    acc = cadd<float>(acc, cmul<float>(mk<float>(e.x * uscale, e.y * uscale), u));
+                }
+        }
+        a.group[s * n + idx] = acc;
+    }
+}
+
+template <typename K> static int launch_split(K* kern, int* done, const SplitArgs& a, long long ctas, cudaStream_t s)
+{
+    if (ctas <= 0) return GPUFFT_SUCCESS;
+    if (ctas > 0x7fffffffLL) return GPUFFT_ERROR_INVALID_VALUE;
+    const size_t smem = sizeof(cx<float>) * SMEM_ELEMS;
+    int st = ensure_smem(kern, smem, done);
+    if (st) return st;
+    kern<<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
+    return check_launch();
+}
+
+template <int L, bool SINGLE, int K> static int launch_mid_k(const SplitArgs& a, long long ctas, cudaStream_t s)
+{
+    static int done[64] = {0};
+    return launch_split(split_mid<L, SINGLE, K>, done, a, ctas, s);
+}
+
+// one-kernel products for rings N <= 8192 (transform length 2^L, L = 1..12),
+// compiled in separate translation units by L range
+int launch_split_single_lo(int L, const SplitArgs& a, long long ctas, cudaStream_t s);  // L 1..6
+int launch_split_single_mid(int L, const SplitArgs& a, long long ctas, cudaStream_t s); // L 7..9
+int launch_split_single_hi(int L, const SplitArgs& a, long long ctas, cudaStream_t s);  // L 10..12
+
+} // namespace gfb

@@ -127,10 +127,12 @@ int gpufft_host_ffnt_tables_f64(int n, void* roots, void* inv_roots, void* twist
 /* ------------------------------------------------------------------------ */
 
 /* Number of complex entries of the native FFNT twiddle block for N = 2^n_power:
- * [roots N/4 | inverse roots N/4 | twist N/2 | untwist N/2] (0 if out of range,
- * n_power in [2, 25]). Same values as FFNT<T>::ReverseRootTable_ffnt,
- * InverseReverseRootTable_ffnt, twist_table_ffnt, untwist_table_ffnt
- * (reference fft_cpu.cu:435-473), computed on the device with sincospi. */
+ * [roots N/4 | inverse roots N/4 | twist N/2 | untwist N/2 | U N/2] (0 if out of
+ * range, n_power in [2, 25]). The first four hold the values of
+ * FFNT<T>::ReverseRootTable_ffnt, InverseReverseRootTable_ffnt,
+ * twist_table_ffnt, untwist_table_ffnt (reference fft_cpu.cu:435-473); U is
+ * the transform of the all-ones polynomial (used by the split product). All
+ * are computed on the device with sincospi. */
 size_t gpufft_ffnt_tables_count(int n_power);
 int gpufft_ffnt_make_tables_f32(int n_power, void* tables, gpufft_stream_t stream);
 int gpufft_ffnt_make_tables_f64(int n_power, void* tables, gpufft_stream_t stream);
@@ -148,6 +150,64 @@ int gpufft_negacyclic_mul_f32(const float* a, const float* b, float* c, int n_po
 int gpufft_negacyclic_mul_f64(const double* a, const double* b, double* c, int n_power, int batch,
                               const void* tables, void* workspace, size_t workspace_bytes,
                               gpufft_stream_t stream);
+
+/* Linear product of real polynomials, the product the reference forms with
+ * GPU_FFT R_R on zero-padded inputs (reference fft.cu:600-725, example
+ * test_fft_gpu_R_R.cu:153-164): c[k] = a[k] * b[k], a and b rows of
+ * N = 2^n_power (n_power in [1, 21]), c rows of 2N (the last entry is 0).
+ * `tables` is the native block for the ring 2N (gpufft_ffnt_make_tables_* with
+ * n_power + 1). Computed as a negacyclic product of length 2N whose zero upper
+ * halves make each operand a real half-length transform. Not rounded. */
+size_t gpufft_linear_mul_workspace_bytes(int n_power, int batch, int precision_bits);
+int gpufft_linear_mul_f32(const float* a, const float* b, float* c, int n_power, int batch, const void* tables,
+                          void* workspace, size_t workspace_bytes, gpufft_stream_t stream);
+int gpufft_linear_mul_f64(const double* a, const double* b, double* c, int n_power, int batch,
+                          const void* tables, void* workspace, size_t workspace_bytes, gpufft_stream_t stream);
+
+/* Vector-Jacobian product of gpufft_linear_mul_f32 (no reference counterpart):
+ * for an upstream gradient g (rows of 2N), grad_a[i] = sum_k g[k] b[k-i] and
+ * grad_b[j] = sum_k g[k] a[k-j] (rows of N), computed as the correlation
+ * IFFT(G conj(B)), IFFT(G conj(A)) through the same fused transform chain.
+ * n_power in [1, 20]; tables as for gpufft_linear_mul_f32. */
+size_t gpufft_linear_mul_vjp_workspace_bytes(int n_power, int batch);
+int gpufft_linear_mul_vjp_f32(const float* g, const float* a, const float* b, float* grad_a, float* grad_b,
+                              int n_power, int batch, const void* tables, void* workspace, size_t workspace_bytes,
+                              gpufft_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched products of mixed ring sizes (no reference counterpart: the      */
+/* reference runs one ring size per call). One plan holds the twiddles,      */
+/* workspace and work lists of a fixed list of requests; execution is one    */
+/* persistent cooperative launch (capturable in a CUDA graph).               */
+/* ------------------------------------------------------------------------ */
+typedef struct gpufft_batch_plan_s* gpufft_batch_plan;
+
+/* Plan for `count` negacyclic products with rings N_i = 2^n_powers[i]
+ * (n_powers in [2, 17]); precision_bits 64 (double) or 32 (float). Allocates
+ * the plan's device memory (tables, workspace); synchronises `stream`. */
+int gpufft_batch_plan_create(gpufft_batch_plan* plan, const int* n_powers, int count, int precision_bits,
+                             gpufft_stream_t stream);
+/* The packed layout the plan expects for a, b and c: requests grouped by ring
+ * size. order[k] is the request stored k-th, offsets[i] the coefficient offset
+ * of request i in the packed arrays, *total their length. Any may be NULL. */
+int gpufft_batch_plan_layout(gpufft_batch_plan plan, int* order, long long* offsets, long long* total);
+/* c = a * b for every request, in one persistent launch on `stream`. */
+int gpufft_batch_plan_execute(gpufft_batch_plan plan, const void* a, const void* b, void* c, gpufft_stream_t stream);
+/* Time the candidate launch shapes (CTAs per SM, work items per grab) on these
+ * buffers and keep the fastest; cache_path (may be NULL) is a JSON-lines file
+ * of earlier results keyed by GPU, driver, precision and size histogram. */
+int gpufft_batch_plan_autotune(gpufft_batch_plan plan, const void* a, const void* b, void* c,
+                               const char* cache_path, gpufft_stream_t stream);
+/* Capture one execution on these buffers into a CUDA graph held by the plan
+ * (stream must be a non-default stream), then launch it with _replay. */
+int gpufft_batch_plan_capture(gpufft_batch_plan plan, const void* a, const void* b, void* c, gpufft_stream_t stream);
+int gpufft_batch_plan_replay(gpufft_batch_plan plan, gpufft_stream_t stream);
+/* Launch shape in use, grid size of the last launch, workspace size. */
+int gpufft_batch_plan_info(gpufft_batch_plan plan, int* ctas_per_sm, int* items_per_grab, int* grid,
+                           long long* workspace_bytes);
+/* Reads and clears the plan's barrier-timeout flag (synchronous). */
+int gpufft_batch_plan_status(gpufft_batch_plan plan, int* barrier_timeouts);
+int gpufft_batch_plan_destroy(gpufft_batch_plan plan);
 
 /* Allocation-free gpufft_negacyclic_mul_f64, for callers that cannot call
  * cudaMalloc (code running inside another runtime's device memory pool, plugin

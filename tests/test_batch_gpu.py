@@ -1,0 +1,86 @@
+"""GPU tests of the mixed-size batch plan (config 4 of the workload list):
+requests with ring sizes 2^10 .. 2^17 run in one persistent cooperative launch
+(captured in a CUDA graph) and must give outputs identical to per-size
+sequential launches of gpufft_negacyclic_mul_*; FP64 results of 16-bit
+coefficients are exact."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def make_requests(rng, count, lo=10, hi=17):
+    return [int(x) for x in rng.integers(lo, hi + 1, count)]
+
+
+def per_size_reference(gf, plan, a_list, b_list, dtype):
+    # one negacyclic_mul call per ring size on the same data
+    out = [None] * len(a_list)
+    sizes = sorted(set(plan.n_powers))
+    for np_ in sizes:
+        idx = [i for i, n in enumerate(plan.n_powers) if n == np_]
+        A = torch.stack([a_list[i] for i in idx])
+        B = torch.stack([b_list[i] for i in idx])
+        C = gf.negacyclic_mul(A, B)
+        for k, i in enumerate(idx):
+            out[i] = C[k]
+    return out
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_batch_matches_per_size_launches(gf, O, dev, dtype):
+    rng = np.random.default_rng(44)
+    n_powers = make_requests(rng, 96, 2, 17)
+    plan = gf.BatchPlan(n_powers, dtype)
+    a_list = [torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, 1 << n).astype(np.float64)).to(dev, dtype)
+              for n in n_powers]
+    b_list = [torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, 1 << n).astype(np.float64)).to(dev, dtype)
+              for n in n_powers]
+    a, b = plan.pack(a_list), plan.pack(b_list)
+    c = plan.execute(a, b)
+    ref = per_size_reference(gf, plan, a_list, b_list, dtype)
+    got = plan.unpack(c)
+    for i in range(len(n_powers)):
+        assert torch.equal(got[i], ref[i]), (i, n_powers[i])
+    assert plan.status() == 0
+    if dtype == torch.float64:  # |c| < 2^47: exact
+        for i in rng.choice(len(n_powers), 6, replace=False):
+            n = 1 << n_powers[i]
+            ai = a_list[i].cpu().numpy().astype(np.int64)
+            bi = b_list[i].cpu().numpy().astype(np.int64)
+            idx = np.sort(rng.choice(n, min(n, 64), replace=False)).astype(np.int32)
+            want = O.wrap64(O.negacyclic_coeffs(ai, bi, idx))
+            assert np.array_equal(np.rint(got[i].cpu().numpy()[idx]).astype(np.int64), want)
+    plan.close()
+
+
+def test_batch_config4_graph_and_autotune(gf, dev):
+    # config 4: 4096 requests, ring sizes log-uniform over 2^10..2^17, FP64,
+    # one persistent launch captured in a CUDA graph, autotuned launch shape
+    rng = np.random.default_rng(4)
+    n_powers = make_requests(rng, 4096)
+    plan = gf.BatchPlan(n_powers, torch.float64)
+    g = torch.Generator(device=dev).manual_seed(4)
+    a = torch.randint(-(1 << 15), 1 << 15, (plan.total,), device=dev, generator=g).double()
+    b = torch.randint(-(1 << 15), 1 << 15, (plan.total,), device=dev, generator=g).double()
+    c0 = plan.execute(a, b)
+    with tempfile.TemporaryDirectory() as d:
+        cache = os.path.join(d, "tune.jsonl")
+        info = plan.autotune(a, b, torch.empty_like(a), cache)
+        assert info["ctas_per_sm"] in (1, 2) and info["items_per_grab"] in (1, 2, 4)
+        assert os.path.exists(cache)
+        plan.autotune(a, b, torch.empty_like(a), cache)  # cache hit
+    s = torch.cuda.Stream()
+    c1 = torch.full_like(a, float("nan"))
+    torch.cuda.synchronize()
+    plan.capture(a, b, c1, s)
+    plan.replay(s)
+    plan.replay(s)
+    s.synchronize()
+    assert torch.equal(c0, c1)
+    assert plan.status() == 0
+    plan.close()

@@ -25,7 +25,15 @@ def test_device_tables_match_reference_values(gf, O, dev, T, n_power):
     np.testing.assert_allclose(t[: M // 2], r[: M // 2], rtol=0, atol=tol)
     np.testing.assert_allclose(t[M // 2: M], ri[: M // 2], rtol=0, atol=tol)
     np.testing.assert_allclose(t[M: 2 * M], tw, rtol=0, atol=tol)
-    np.testing.assert_allclose(t[2 * M:], utw, rtol=0, atol=tol)
+    np.testing.assert_allclose(t[2 * M: 3 * M], utw, rtol=0, atol=tol)
+    # U: transform of the all-ones polynomial in output (bit-reversed) order
+    br = np.array([O.lib().orc_bitreverse(i, n_power - 1) for i in range(M)]) if M > 1 else np.zeros(1, int)
+    x = (1 + 1j) * np.exp(1j * np.pi * np.arange(M) / n)
+    want_u = (M * np.fft.ifft(x))[br]
+    # (numpy's own FFT of length M carries ~1e-16 * M absolute error)
+    scale = np.max(np.abs(want_u))
+    np.testing.assert_allclose(t[3 * M:], want_u, rtol=1e-6 if T == "f32" else 1e-11,
+                               atol=(1e-6 if T == "f32" else 1e-13) * scale)
 
 
 @pytest.mark.parametrize("n_power,batch", [(2, 5), (3, 3), (10, 9), (12, 3), (13, 5), (14, 2), (15, 3), (16, 3),
