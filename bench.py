@@ -121,6 +121,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def reduce_max(value, dist, device):
+    """Max of a per-rank float over all ranks (the whole-job step time)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_inputs(batch, n, rank):
     import torch
     g = torch.Generator().manual_seed(SEED + rank)
@@ -472,11 +482,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(ms):
-        if dist is None:
-            return ms
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(ms, dist, dev)
 
     peak, peak_kind = peaks()
     if args.path in ("batch", "vjp"):

@@ -87,6 +87,27 @@ def ref():
     return _REF
 
 
+_REFGPU = None
+
+
+def ref_gpu():
+    """The reference's own GPU library (src/lib/fft.cu compiled for sm_100a by
+    oracle/Makefile), or None where it was never compiled."""
+    global _REFGPU
+    if _REFGPU is None:
+        path = os.path.join(HERE, "_ref", "libgpufft_ref_gpu.so")
+        if not os.path.exists(path):
+            return None
+        R = ctypes.CDLL(path)
+        vp, i, d, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float
+        R.ref_gpu_ffnt_f64.argtypes = [vp, vp, vp, vp, i, i, d, d, i, i, vp]
+        R.ref_gpu_ffnt_f32.argtypes = [vp, vp, vp, vp, i, i, f, f, i, i, vp]
+        R.ref_gpu_fft_c2c_f64.argtypes = [vp, vp, i, i, i, d, d, i, i, vp]
+        R.ref_gpu_fft_r2r_f64.argtypes = [vp, vp, vp, i, i, i, d, d, i, i, vp]
+        _REFGPU = R
+    return _REFGPU
+
+
 def _np(dtype):
     return np.float64 if dtype in ("f64", np.float64) else np.float32
 
