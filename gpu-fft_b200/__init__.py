@@ -108,6 +108,13 @@ def lib() -> ctypes.CDLL:
         L.gpufft_negacyclic_mul_split_workspace_bytes.argtypes = [i, i, i]
         L.gpufft_negacyclic_mul_split_workspace_bytes.restype = sz
         L.gpufft_negacyclic_mul_split_f32.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, vp, sz, vp, vp]
+        L.gpufft_negacyclic_mul_host_workspace_bytes.argtypes = [i, i, i, i]
+        L.gpufft_negacyclic_mul_host_workspace_bytes.restype = sz
+        L.gpufft_negacyclic_mul_f32_host.argtypes = [vp, vp, vp, i, i, i, vp, vp, sz, vp]
+        L.gpufft_negacyclic_mul_f64_host.argtypes = [vp, vp, vp, i, i, i, vp, vp, sz, vp]
+        L.gpufft_negacyclic_mul_split_f32_host_workspace_bytes.argtypes = [i, i, i, i]
+        L.gpufft_negacyclic_mul_split_f32_host_workspace_bytes.restype = sz
+        L.gpufft_negacyclic_mul_split_f32_host.argtypes = [vp, vp, vp, i, i, i, i, i, i, i, vp, vp, sz, vp, vp]
         L.gpufft_last_cuda_error.restype = i
         L.gpufft_status_string.restype = ctypes.c_char_p
         L.gpufft_status_string.argtypes = [i]
@@ -312,6 +319,76 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
         _ptr(tables), workspace.data_ptr(), workspace.numel() * workspace.element_size(), err.data_ptr(),
         _stream_handle(stream))
     check(st, "negacyclic_mul_split")
+    return (out, err) if return_error else out
+
+
+def _host_operands(a, b, dtypes, what):
+    import torch
+    if a.device.type != "cpu" or b.device.type != "cpu":
+        raise GpufftError(ERROR_INVALID_VALUE, f"{what}: a and b must be host tensors")
+    if a.dim() != 2 or b.shape != a.shape or a.dtype not in dtypes or b.dtype != a.dtype:
+        raise GpufftError(ERROR_INVALID_VALUE, f"{what}: a and b must be (batch, 2^k) tensors of one supported dtype")
+    if not (a.is_contiguous() and b.is_contiguous()):
+        raise GpufftError(ERROR_INVALID_VALUE, f"{what}: a and b must be contiguous")
+    batch, n = a.shape
+    n_power = n.bit_length() - 1
+    if (1 << n_power) != n:
+        raise GpufftError(ERROR_INVALID_VALUE, f"{what}: rows must have 2^k entries")
+    return batch, n, n_power
+
+
+def negacyclic_mul_host(a, b, out=None, tables=None, workspace=None, chunk=0, device=None, stream=None):
+    """negacyclic_mul on HOST tensors (pin them for overlap): chunks are copied in,
+    multiplied and copied out with the transfers overlapping the computation.
+    Asynchronous on `stream` like the device call; synchronise before reading out."""
+    import torch
+    batch, n, n_power = _host_operands(a, b, (torch.float32, torch.float64), "negacyclic_mul_host")
+    f64 = a.dtype == torch.float64
+    dev = torch.device(device) if device is not None else (tables.device if tables is not None else
+                                                            torch.device("cuda", torch.cuda.current_device()))
+    if tables is None:
+        tables = ffnt_tables(n_power, "f64" if f64 else "f32", dev, stream)
+    if out is None:
+        out = torch.empty((batch, n), dtype=a.dtype, pin_memory=True)
+    L = lib()
+    need = int(L.gpufft_negacyclic_mul_host_workspace_bytes(n_power, batch, int(chunk), 64 if f64 else 32))
+    if need == 0:
+        raise ValueError("Invalid n_power range!")
+    if workspace is None:
+        workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+    f = L.gpufft_negacyclic_mul_f64_host if f64 else L.gpufft_negacyclic_mul_f32_host
+    check(f(a.data_ptr(), b.data_ptr(), out.data_ptr(), n_power, batch, int(chunk), _ptr(tables),
+            workspace.data_ptr(), workspace.numel() * workspace.element_size(), _stream_handle(stream)),
+          "negacyclic_mul_host")
+    return out
+
+
+def negacyclic_mul_split_host(a, b, out=None, input_bits=24, non_negative=False, limbs=None, tables=None,
+                              workspace=None, chunk=0, device=None, stream=None, return_error=False):
+    """negacyclic_mul_split on HOST int32 tensors (pin them for overlap), chunked with
+    the transfers overlapping the computation; int64 host result. Asynchronous on
+    `stream`; synchronise before reading out (or the error)."""
+    import torch
+    batch, n, n_power = _host_operands(a, b, (torch.int32,), "negacyclic_mul_split_host")
+    dev = torch.device(device) if device is not None else (tables.device if tables is not None else
+                                                            torch.device("cuda", torch.cuda.current_device()))
+    w, k = limbs if limbs is not None else split_plan(n_power, input_bits, non_negative)
+    if tables is None:
+        tables = ffnt_tables(n_power, "f32", dev, stream)
+    if out is None:
+        out = torch.empty((batch, n), dtype=torch.int64, pin_memory=True)
+    L = lib()
+    need = int(L.gpufft_negacyclic_mul_split_f32_host_workspace_bytes(n_power, batch, int(chunk), k))
+    if need == 0:
+        raise ValueError("Invalid n_power range!")
+    if workspace is None:
+        workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+    err = torch.zeros(1, dtype=torch.float32, device=dev)
+    check(L.gpufft_negacyclic_mul_split_f32_host(
+        a.data_ptr(), b.data_ptr(), out.data_ptr(), n_power, batch, int(chunk), int(input_bits),
+        int(bool(non_negative)), w, k, _ptr(tables), workspace.data_ptr(),
+        workspace.numel() * workspace.element_size(), err.data_ptr(), _stream_handle(stream)),
+        "negacyclic_mul_split_host")
     return (out, err) if return_error else out
 
 

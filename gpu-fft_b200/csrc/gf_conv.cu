@@ -54,6 +54,7 @@ template <int L, bool SINGLE> __global__ void __launch_bounds__(NTHR, 1) vjp_ker
     {
         const Tile<L, false, W0> tl(a.geo, cta, t);
         c.g = tl.g;
+        c.vec = tw_vec_ok<float>(a.roots) && tw_vec_ok<float>(a.inv_roots);
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {

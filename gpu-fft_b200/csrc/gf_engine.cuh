@@ -71,7 +71,14 @@ struct TwCtx
     long long g; // group of this CTA's sub-networks at the first stage of the pass
     int s0;      // first stage of the pass
     int neg;     // negacyclic (X^N+1) twiddle indexing
+    int vec = 0; // float tables on a 16-byte boundary: load twiddle pairs as float4
 };
+
+// Twiddle-table base suitable for paired (16-byte) loads.
+template <typename T> __device__ __forceinline__ int tw_vec_ok(const cx<T>* tw)
+{
+    return sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(tw) & 15) == 0;
+}
 
 // One round: radix-2^RB network on window bits [A, A+RB) of the registers, for
 // NA arrays that share placement and twiddles. All twiddles of the round are
@@ -91,12 +98,26 @@ __device__ __forceinline__ void round_net(cx<T> (&x)[NA][RPT], const cx<T>* __re
         const int nhi = A + RB - 1 - pb;
         const int u = QOFF + L - 1 - (W + pb);
         const long long gbase = (c.g << u) + (c.neg ? (1LL << (c.s0 + u)) : 0LL);
-#pragma unroll
-        for (int h = 0; h < (1 << nhi); h++)
+        // The 2^nhi twiddles of this step are consecutive table entries
+        // idx0 + h, and idx0 is a multiple of 2^nhi: the register bits above
+        // pb are the lowest bits of the group index, and e_base leaves the
+        // window's bits clear.
+        const cx<T>* p0 = tw + gbase + (((eb >> QOFF) & qmask) >> (L - u));
+        cx<T>* wk = w + (1 << nhi) - 1;
+        if (sizeof(T) == 4 && nhi >= 1 && c.vec)
         {
-            const int e = eb | ((h << (pb + 1)) << W);
-            const int q = (e >> QOFF) & qmask;
-            w[(1 << nhi) - 1 + h] = ldg<T>(tw + gbase + (q >> (L - u)));
+#pragma unroll
+            for (int h = 0; h < (1 << nhi); h += 2)
+            {
+                const float4 v = __ldg(reinterpret_cast<const float4*>(p0 + h));
+                wk[h] = mk<T>((T)v.x, (T)v.y);
+                wk[h + 1] = mk<T>((T)v.z, (T)v.w);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int h = 0; h < (1 << nhi); h++) wk[h] = ldg<T>(p0 + h);
         }
     }
 #pragma unroll

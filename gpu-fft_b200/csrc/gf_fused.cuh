@@ -42,6 +42,7 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
     {
         const Tile<L, false, W0> tl(a.geo, cta, t);
         c.g = tl.g;
+        c.vec = tw_vec_ok<T>(a.roots) && tw_vec_ok<T>(a.inv_roots);
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {

@@ -277,6 +277,12 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
     constexpr int QOFF = STRIDED ? EBITS - L : 0;
     using S = Sched<QOFF, L>;
     constexpr int W0 = S::win(0, FWD), WL = S::win(S::n - 1, FWD);
+    // A round in window 0 keeps 16 consecutive elements in each thread, so a
+    // warp's access would touch 32 separate sectors. Such passes load (store)
+    // in window 8, where the thread index runs along the lowest element bits,
+    // and move to (from) window 0 with one more shared-memory transpose.
+    constexpr int WIN = W0 == 0 ? 8 : W0;
+    constexpr int WOUT = WL == 0 ? 8 : WL;
     const int t = threadIdx.x;
     // the tile lies in one batch entry: strided passes, and contiguous passes of
     // transforms with at least ECTA elements
@@ -285,7 +291,7 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
     cx<T> x[1][RPT];
     TwCtx c;
     {
-        const Tile<L, STRIDED, W0> tl(a.geo, cta, t);
+        const Tile<L, STRIDED, WIN> tl(a.geo, cta, t);
         c.g = tl.g;
         const int kind = a.in_kind;
         const bool real_rows_kind = kind == IN_FOLD || kind == IN_FOLD2 || kind == IN_LIN2 || kind == IN_VJP3;
@@ -323,9 +329,12 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
     }
     c.s0 = a.geo.s0;
     c.neg = a.geo.neg;
+    c.vec = tw_vec_ok<T>(a.table);
+    if constexpr (WIN != W0) transpose<T, WIN, W0, 1>(x, sm, t);
     run_rounds<T, FWD, QOFF, L, 1>(x, sm, a.table, c, t);
+    if constexpr (WOUT != WL) transpose<T, WL, WOUT, 1>(x, sm, t);
     {
-        const Tile<L, STRIDED, WL> tl(a.geo, cta, t);
+        const Tile<L, STRIDED, WOUT> tl(a.geo, cta, t);
         const int kind = a.out_kind;
         if (one_entry && tl.b[0] < a.batch && (kind == OUT_UNFOLD || kind == OUT_CPX))
         {
@@ -360,8 +369,12 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
     }
 }
 
+// Resident CTAs per SM the pass kernels are compiled for: float passes hold 32
+// data registers per thread and fit three CTAs; double passes fit two.
+template <typename T> constexpr int pass_min_blocks() { return sizeof(T) == 4 ? 3 : 2; }
+
 template <typename T, bool FWD, int L, bool STRIDED>
-__global__ void __launch_bounds__(NTHR, 2) pass_kernel(const PassArgs<T> a)
+__global__ void __launch_bounds__(NTHR, pass_min_blocks<T>()) pass_kernel(const PassArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     pass_body<T, FWD, L, STRIDED>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));

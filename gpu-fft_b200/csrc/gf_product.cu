@@ -252,6 +252,68 @@ extern "C" int gpufft_negacyclic_mul_f64(const double* a, const double* b, doubl
 }
 
 // ---------------------------------------------------------------------------
+// Host-buffer variants: a, b, c in (page-locked) host memory, chunks of the
+// batch staged through the workspace with the transfers overlapped
+// (gf_pipe.cuh). Workspace = staging slots, then the product workspace of
+// one chunk.
+// ---------------------------------------------------------------------------
+#include "gf_pipe.cuh"
+
+namespace gfb
+{
+static long long host_chunk(int n_power, long long batch, long long chunk, size_t cxb)
+{
+    if (chunk > 0) return chunk < batch ? chunk : batch;
+    return pipe_chunk(wave_products(n_power, batch, cxb), batch);
+}
+
+template <typename T>
+static int negacyclic_mul_host(const T* a, const T* b, T* c, int n_power, int batch, int chunk, const void* tables,
+                               void* ws, size_t ws_bytes, cudaStream_t s)
+{
+    if (n_power < NATIVE_MIN_NPOWER || n_power > NATIVE_MAX_NPOWER) return GPUFFT_ERROR_INVALID_N_POWER;
+    if (batch <= 0) return GPUFFT_ERROR_INVALID_VALUE;
+    const long long ch = host_chunk(n_power, batch, chunk, sizeof(cx<T>));
+    const size_t row = sizeof(T) << n_power;
+    const size_t slots = pipe_bytes(ch, row, row);
+    if (!ws || ws_bytes < slots) return GPUFFT_ERROR_WORKSPACE;
+    void* pws = static_cast<char*>(ws) + slots;
+    const size_t pws_bytes = ws_bytes - slots;
+    return run_pipeline(a, b, c, batch, ch, row, row, ws, slots, s,
+                        [&](void* da, void* db, void* dc, long long rows, cudaStream_t st) {
+                            return negacyclic_mul<T>(static_cast<const T*>(da), static_cast<const T*>(db),
+                                                     static_cast<T*>(dc), n_power, (int)rows, tables, pws, pws_bytes,
+                                                     st);
+                        });
+}
+} // namespace gfb
+
+extern "C" size_t gpufft_negacyclic_mul_host_workspace_bytes(int n_power, int batch, int chunk, int precision_bits)
+{
+    if (n_power < gfb::NATIVE_MIN_NPOWER || n_power > gfb::NATIVE_MAX_NPOWER || batch <= 0) return 0;
+    if (precision_bits != 32 && precision_bits != 64) return 0;
+    const size_t cxb = precision_bits == 64 ? 16 : 8;
+    const long long ch = gfb::host_chunk(n_power, batch, chunk, cxb);
+    const size_t row = (cxb / 2) << n_power;
+    return gfb::pipe_bytes(ch, row, row) + gpufft_negacyclic_mul_workspace_bytes(n_power, (int)ch, precision_bits);
+}
+
+extern "C" int gpufft_negacyclic_mul_f32_host(const float* a, const float* b, float* c, int n_power, int batch,
+                                              int chunk, const void* tables, void* workspace, size_t workspace_bytes,
+                                              gpufft_stream_t stream)
+{
+    return gfb::negacyclic_mul_host<float>(a, b, c, n_power, batch, chunk, tables, workspace, workspace_bytes,
+                                           (cudaStream_t)stream);
+}
+extern "C" int gpufft_negacyclic_mul_f64_host(const double* a, const double* b, double* c, int n_power, int batch,
+                                              int chunk, const void* tables, void* workspace, size_t workspace_bytes,
+                                              gpufft_stream_t stream)
+{
+    return gfb::negacyclic_mul_host<double>(a, b, c, n_power, batch, chunk, tables, workspace, workspace_bytes,
+                                            (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free variant of gpufft_negacyclic_mul_f64.
 //
 // Some callers cannot call cudaMalloc at all: code running where the CUDA

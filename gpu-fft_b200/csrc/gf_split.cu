@@ -1,6 +1,7 @@
 // gpufft-b200: FP32 split-precision negacyclic product -- host side (plans,
 // workspace, launches) and the C ABI. The kernels are in gf_split.cuh.
 #include "gf_split.cuh"
+#include "gf_pipe.cuh"
 
 namespace gfb
 {
@@ -95,7 +96,7 @@ template <int L> static int launch_inv0(const SplitArgs& a, long long ctas, cuda
 
 static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch, int input_bits,
                      int non_negative, int limb_bits, int num_limbs, const void* tables, void* ws, size_t ws_bytes,
-                     unsigned* max_err, cudaStream_t s)
+                     unsigned* max_err, cudaStream_t s, bool reset_err = true)
 {
     if (n_power < 2 || n_power > 22) return GPUFFT_ERROR_INVALID_N_POWER;
     if (!a || !b || !c || !tables || batch <= 0 || input_bits < 1 || input_bits > 31) return GPUFFT_ERROR_INVALID_VALUE;
@@ -132,7 +133,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
     const size_t need1 = split_ws_bytes(m, k, 1);
     if (!ws || ws_bytes < need1) return GPUFFT_ERROR_WORKSPACE;
     if (split_ws_bytes(m, k, W) > ws_bytes) W = (long long)(ws_bytes / need1);
-    if (max_err)
+    if (max_err && reset_err)
     {
         cudaError_t e = cudaMemsetAsync(max_err, 0, sizeof(unsigned), s);
         if (e != cudaSuccess) return set_cuda_error(e);
@@ -206,6 +207,45 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
     return GPUFFT_SUCCESS;
 }
 
+// Host-buffer variant: chunks staged through the workspace with the transfers
+// overlapped (gf_pipe.cuh); the error report is the maximum over all chunks.
+static long long split_host_chunk(int n_power, int k, long long batch, long long chunk)
+{
+    if (chunk > 0) return chunk < batch ? chunk : batch;
+    return pipe_chunk(split_wave(n_power - 1, k, batch), batch);
+}
+
+static int split_mul_host(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch, int chunk,
+                          int input_bits, int non_negative, int limb_bits, int num_limbs, const void* tables, void* ws,
+                          size_t ws_bytes, unsigned* max_err, cudaStream_t s)
+{
+    if (n_power < 2 || n_power > 22) return GPUFFT_ERROR_INVALID_N_POWER;
+    if (batch <= 0 || input_bits < 1 || input_bits > 31) return GPUFFT_ERROR_INVALID_VALUE;
+    int w = limb_bits, k = num_limbs;
+    if (w <= 0 || k <= 0)
+    {
+        if (!choose_limbs(n_power, input_bits, non_negative != 0, &w, &k)) return GPUFFT_ERROR_INVALID_VALUE;
+    }
+    if (k > SPLIT_MAX_LIMBS) return GPUFFT_ERROR_INVALID_VALUE;
+    const long long ch = split_host_chunk(n_power, k, batch, chunk);
+    const size_t in_row = sizeof(int32_t) << n_power, out_row = sizeof(int64_t) << n_power;
+    const size_t slots = pipe_bytes(ch, in_row, out_row);
+    if (!ws || ws_bytes < slots) return GPUFFT_ERROR_WORKSPACE;
+    if (max_err)
+    {
+        cudaError_t e = cudaMemsetAsync(max_err, 0, sizeof(unsigned), s);
+        if (e != cudaSuccess) return set_cuda_error(e);
+    }
+    void* sws = static_cast<char*>(ws) + slots;
+    const size_t sws_bytes = ws_bytes - slots;
+    return run_pipeline(a, b, c, batch, ch, in_row, out_row, ws, slots, s,
+                        [&](void* da, void* db, void* dc, long long rows, cudaStream_t st) {
+                            return split_mul(static_cast<const int32_t*>(da), static_cast<const int32_t*>(db),
+                                             static_cast<int64_t*>(dc), n_power, (int)rows, input_bits, non_negative,
+                                             w, k, tables, sws, sws_bytes, max_err, st, false);
+                        });
+}
+
 } // namespace gfb
 
 extern "C" int gpufft_split_plan(int n_power, int input_bits, int non_negative, int* limb_bits, int* num_limbs)
@@ -231,4 +271,24 @@ extern "C" int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* 
 {
     return gfb::split_mul(a, b, c, n_power, batch, input_bits, non_negative, limb_bits, num_limbs, tables, workspace,
                           workspace_bytes, reinterpret_cast<unsigned*>(max_error), (cudaStream_t)stream);
+}
+
+extern "C" size_t gpufft_negacyclic_mul_split_f32_host_workspace_bytes(int n_power, int batch, int chunk,
+                                                                       int num_limbs)
+{
+    if (n_power < 2 || n_power > 22 || batch <= 0 || num_limbs < 1 || num_limbs > gfb::SPLIT_MAX_LIMBS) return 0;
+    const long long ch = gfb::split_host_chunk(n_power, num_limbs, batch, chunk);
+    return gfb::pipe_bytes(ch, sizeof(int32_t) << n_power, sizeof(int64_t) << n_power) +
+           gpufft_negacyclic_mul_split_workspace_bytes(n_power, (int)ch, num_limbs);
+}
+
+extern "C" int gpufft_negacyclic_mul_split_f32_host(const int32_t* a, const int32_t* b, int64_t* c, int n_power,
+                                                    int batch, int chunk, int input_bits, int non_negative,
+                                                    int limb_bits, int num_limbs, const void* tables,
+                                                    void* workspace, size_t workspace_bytes, float* max_error,
+                                                    gpufft_stream_t stream)
+{
+    return gfb::split_mul_host(a, b, c, n_power, batch, chunk, input_bits, non_negative, limb_bits, num_limbs, tables,
+                               workspace, workspace_bytes, reinterpret_cast<unsigned*>(max_error),
+                               (cudaStream_t)stream);
 }

@@ -143,6 +143,7 @@ template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const Spl
     c.g = tl.g;
     c.s0 = 0;
     c.neg = 0;
+    c.vec = tw_vec_ok<float>(a.roots) && tw_vec_ok<float>(a.inv_roots);
     const Tile<L, true, WL> to(a.geo, cta, t);
     for (int l = 0; l < a.k; l++)
     {
@@ -183,6 +184,7 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
     c.g = ti.g;
     c.s0 = a.geo.s0;
     c.neg = 0;
+    c.vec = tw_vec_ok<float>(a.roots) && tw_vec_ok<float>(a.inv_roots);
 
     // 1. last forward pass (SINGLE: every forward stage, limb extraction in the
     //    load) of every limb spectrum; results parked in a.spec
@@ -336,6 +338,7 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
     c.g = ti.g;
     c.s0 = 0;
     c.neg = 0;
+    c.vec = tw_vec_ok<float>(a.roots) && tw_vec_ok<float>(a.inv_roots);
     const long long p = ti.b[0];
 
     long long acc_lo[RPT], acc_hi[RPT];

@@ -151,6 +151,20 @@ int gpufft_negacyclic_mul_f64(const double* a, const double* b, double* c, int n
                               const void* tables, void* workspace, size_t workspace_bytes,
                               gpufft_stream_t stream);
 
+/* The same product on HOST buffers (page-locked for overlap): the batch runs in
+ * chunks of `chunk` products (0: the library's choice), each copied in, computed
+ * and copied out on its own streams so that the PCIe transfers of neighbouring
+ * chunks overlap the computation. Ordered after the work queued on `stream`,
+ * and `stream` waits for the last copy: synchronise it before reading c. The
+ * workspace holds three staging slots plus one chunk's product workspace. */
+size_t gpufft_negacyclic_mul_host_workspace_bytes(int n_power, int batch, int chunk, int precision_bits);
+int gpufft_negacyclic_mul_f32_host(const float* a, const float* b, float* c, int n_power, int batch, int chunk,
+                                   const void* tables, void* workspace, size_t workspace_bytes,
+                                   gpufft_stream_t stream);
+int gpufft_negacyclic_mul_f64_host(const double* a, const double* b, double* c, int n_power, int batch, int chunk,
+                                   const void* tables, void* workspace, size_t workspace_bytes,
+                                   gpufft_stream_t stream);
+
 /* Linear product of real polynomials, the product the reference forms with
  * GPU_FFT R_R on zero-padded inputs (reference fft.cu:600-725, example
  * test_fft_gpu_R_R.cu:153-164): c[k] = a[k] * b[k], a and b rows of
@@ -240,6 +254,13 @@ int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* b, int64_t*
                                     int input_bits, int non_negative, int limb_bits, int num_limbs,
                                     const void* tables, void* workspace, size_t workspace_bytes,
                                     float* max_error, gpufft_stream_t stream);
+/* The same product on host buffers, chunked with overlapped transfers exactly
+ * like gpufft_negacyclic_mul_f64_host; max_error (device) covers all chunks. */
+size_t gpufft_negacyclic_mul_split_f32_host_workspace_bytes(int n_power, int batch, int chunk, int num_limbs);
+int gpufft_negacyclic_mul_split_f32_host(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch,
+                                         int chunk, int input_bits, int non_negative, int limb_bits, int num_limbs,
+                                         const void* tables, void* workspace, size_t workspace_bytes,
+                                         float* max_error, gpufft_stream_t stream);
 
 #ifdef __cplusplus
 } /* extern "C" */
