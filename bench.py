@@ -36,7 +36,7 @@ SEED = 20261203 + 3  # config 3 of the workload list
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64", "batch", "vjp"], default="split",

@@ -107,7 +107,10 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
     {
         if (!choose_limbs(n_power, input_bits, non_negative != 0, &w, &k)) return GPUFFT_ERROR_INVALID_VALUE;
     }
-    if (k > SPLIT_MAX_LIMBS || w < 1 || w > 20 || (long long)w * k < input_bits) return GPUFFT_ERROR_INVALID_VALUE;
+    // digits are read from a 64-bit offset value: limbs far above the input
+    // range (w (k-1) >= 48) are rejected
+    if (k > SPLIT_MAX_LIMBS || w < 1 || w > 20 || (long long)w * k < input_bits || w * (k - 1) >= 48)
+        return GPUFFT_ERROR_INVALID_VALUE;
     if (non_negative && input_bits > 30) return GPUFFT_ERROR_INVALID_VALUE;
 
     const int m = n_power - 1;
@@ -128,6 +131,11 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
     A.uspec = tab + 3 * M;
     A.uq = (input_bits - 1) / w;
     A.ur = (input_bits - 1) - w * A.uq;
+    {
+        long long hoff = 0; // 2^(w-1) (1 + 2^w + ... + 2^(w(k-2)))
+        for (int i = 0; i + 1 < k; i++) hoff += 1LL << (w * i + w - 1);
+        A.voff = hoff - A.K;
+    }
 
     long long W = split_wave(m, k, batch);
     const size_t need1 = split_ws_bytes(m, k, 1);
@@ -164,7 +172,20 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         const int L0 = p.L[0];
         // 1. limb extraction + first forward pass (strided), all 2k limbs of a column block
         A.geo = pass_geo(p, 0, m, 0, 2 * wv, &ctas);
-        int st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_fwd0<LL>(A, ctas, s); });
+        int st;
+        if (L0 <= SPLIT_COL_MAX)
+        {
+            const long long threads = 2 * wv * k * (M >> L0);
+            const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
+            st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+                split_fwd0_col<LL><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
+                return check_launch();
+            });
+        }
+        else
+        {
+            st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_fwd0<LL>(A, ctas, s); });
+        }
         if (st) return st;
         // 2. last forward pass of the 2k W limb spectra, in place
         {
@@ -201,7 +222,21 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         }
         // 4. last inverse pass of every group (strided), rounding, int64 recombination
         A.geo = pass_geo(p, 0, m, 0, wv, &ctas);
-        st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_inv0<LL>(A, ctas, s); });
+        if (L0 <= SPLIT_COL_MAX)
+        {
+            const long long threads = wv * (M >> L0);
+            const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
+            st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+                return dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
+                    split_inv0_col<LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
+                    return check_launch();
+                });
+            });
+        }
+        else
+        {
+            st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_inv0<LL>(A, ctas, s); });
+        }
         if (st) return st;
     }
     return GPUFFT_SUCCESS;

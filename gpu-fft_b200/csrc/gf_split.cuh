@@ -38,25 +38,17 @@ namespace gfb
 
 constexpr int SPLIT_MAX_LIMBS = 8;
 
-// Balanced signed digit l (width w, k digits) of v.
-__device__ __forceinline__ int limb_digit(long long v, int l, int w, int k)
+// Balanced signed digits: v = sum_l d_l 2^(w l) with d_l in [-2^(w-1), 2^(w-1))
+// for l < k-1 and the top digit d_(k-1) taking what is left. Digit l is read
+// directly from V = v + voff, where voff = 2^(w-1) (1 + 2^w + ... + 2^(w(k-2))):
+// adding half of every lower digit's range turns the balanced digits into the
+// plain base-2^w digits e_l = d_l + 2^(w-1) of V, so
+// d_l = ((V >> wl) mod 2^w) - 2^(w-1) for l < k-1, and the top digit is
+// V >> w(k-1) (arithmetic shift).
+__device__ __forceinline__ int split_digit(long long V, int l, int w, int k)
 {
-    const long long base = 1LL << w, half = base >> 1;
-    long long d = 0;
-    for (int i = 0; i <= l; i++)
-    {
-        if (i == k - 1)
-        {
-            d = v;
-        }
-        else
-        {
-            const long long r = v & (base - 1);
-            d = (r >= half) ? r - base : r;
-        }
-        v = (v - d) >> w;
-    }
-    return (int)d;
+    if (l == k - 1) return (int)(V >> (w * l));
+    return (int)((V >> (w * l)) & ((1LL << w) - 1)) - (1 << (w - 1));
 }
 
 struct SplitArgs
@@ -73,6 +65,7 @@ struct SplitArgs
     unsigned* max_err; // float bits of the largest pre-rounding error (may be null)
     const cx<float>* uspec; // transform of the all-ones polynomial (table block)
     long long K;       // centring offset subtracted from every coefficient (0: none)
+    long long voff;    // split_digit offset minus K: V = x + voff for a raw coefficient x
     int uq, ur;        // K = 2^(w uq + ur): centring term joins groups s = l + uq, scaled 2^ur
     float scale;
     int w, k;
@@ -136,8 +129,8 @@ template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const Spl
 #pragma unroll
     for (int r = 0; r < RPT; r++)
     {
-        vlo[r] = (int)((long long)__ldcs(src + tl.j[r]) - a.K);
-        vhi[r] = (int)((long long)__ldcs(src + tl.j[r] + M) - a.K);
+        vlo[r] = __ldcs(src + tl.j[r]);
+        vhi[r] = __ldcs(src + tl.j[r] + M);
     }
     TwCtx c;
     c.g = tl.g;
@@ -151,7 +144,8 @@ template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const Spl
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            const cx<float> f = mk<float>((float)limb_digit(vlo[r], l, a.w, a.k), (float)limb_digit(vhi[r], l, a.w, a.k));
+            const cx<float> f = mk<float>((float)split_digit((long long)vlo[r] + a.voff, l, a.w, a.k),
+                                          (float)split_digit((long long)vhi[r] + a.voff, l, a.w, a.k));
             x[0][r] = cmul<float>(f, ldg<float>(a.twist + tl.j[r]));
         }
         if (l > 0) __syncthreads();
@@ -203,8 +197,8 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
             if (SINGLE)
             {
                 const int32_t* src = (op == 0 ? a.a : a.b) + ti.b[r] * 2 * M + ti.j[r];
-                const long long v0 = (long long)__ldg(src) - a.K, v1 = (long long)__ldg(src + M) - a.K;
-                const cx<float> f = mk<float>((float)limb_digit(v0, l, a.w, K), (float)limb_digit(v1, l, a.w, K));
+                const long long v0 = (long long)__ldg(src) + a.voff, v1 = (long long)__ldg(src + M) + a.voff;
+                const cx<float> f = mk<float>((float)split_digit(v0, l, a.w, K), (float)split_digit(v1, l, a.w, K));
                 x[0][r] = cmul<float>(f, ldg<float>(a.twist + ti.j[r]));
             }
             else
@@ -373,6 +367,119 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
         __stcs(reinterpret_cast<long long*>(dst + te.j[r] + M), acc_hi[r] + uu_term(a, te.j[r] + M, 2 * M));
     }
     report_err(a.max_err, err);
+}
+
+// --------------------------------------------------------------------------
+// Column kernels for short first/last passes (L0 <= 4 stages, rings up to
+// N = 2^17): the stages [0, L0) of a 2^m transform are closed 2^L0-point
+// networks on the columns c of the M / 2^L0 x 2^L0 view, j = c + i C
+// (C = 2^(m-L0)). One thread owns one column (of one limb, or of one product
+// for the inverse) in registers: no shared memory, no barriers, coalesced
+// across the warp, and many more threads in flight than 4096-element tiles.
+// Stage s pairs i with i + 2^(L0-1-s) and uses table[i >> (L0-s)] -- the same
+// butterflies, twiddles and order as the engine's pass, so the values are
+// identical.
+// --------------------------------------------------------------------------
+constexpr int SPLIT_COL_MAX = 4;
+constexpr int SPLIT_COL_THREADS = 128;
+
+template <int L0> __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitArgs a)
+{
+    constexpr int R = 1 << L0;
+    const int m = a.geo.m;
+    const long long M = 1LL << m, C = M >> L0;
+    const long long idx = (long long)blockIdx.x * SPLIT_COL_THREADS + threadIdx.x;
+    // thread order: column fastest, then limb, then (operand, product)
+    const long long c = idx & (C - 1);
+    const long long rest = idx >> (m - L0);
+    const long long bb = rest / a.k;
+    const int l = (int)(rest - bb * a.k);
+    if (bb >= 2 * a.W) return;
+    const long long op = bb / a.W, p = bb - op * a.W;
+    const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M + c;
+    cx<float> x[R];
+#pragma unroll
+    for (int i = 0; i < R; i++)
+    {
+        const long long V0 = (long long)__ldg(src + i * C) + a.voff;
+        const long long V1 = (long long)__ldg(src + i * C + M) + a.voff;
+        const cx<float> f = mk<float>((float)split_digit(V0, l, a.w, a.k), (float)split_digit(V1, l, a.w, a.k));
+        x[i] = cmul<float>(f, ldg<float>(a.twist + c + i * C));
+    }
+#pragma unroll
+    for (int s = 0; s < L0; s++)
+    {
+        const int h = 1 << (L0 - 1 - s);
+#pragma unroll
+        for (int i = 0; i < R; i++)
+            if (!(i & h)) ct_bfly<float>(x[i], x[i + h], ldg<float>(a.roots + (i >> (L0 - s))));
+    }
+    cx<float>* dst = a.spec + ((op * a.k + l) * a.W + p) * M + c;
+#pragma unroll
+    for (int i = 0; i < R; i++) dst[i * C] = x[i];
+}
+
+template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_inv0_col(const SplitArgs a)
+{
+    constexpr int R = 1 << L0;
+    const int m = a.geo.m;
+    const long long M = 1LL << m, C = M >> L0;
+    const long long idx = (long long)blockIdx.x * SPLIT_COL_THREADS + threadIdx.x;
+    const long long c = idx & (C - 1);
+    const long long p0 = idx >> (m - L0);
+    // the grid covers W C threads exactly (C is a multiple of the block size);
+    // out-of-range threads still reach report_err's warp shuffle
+    const bool ok = p0 < a.W;
+    const long long p = ok ? p0 : 0;
+    cx<float> un[R];
+#pragma unroll
+    for (int i = 0; i < R; i++)
+    {
+        const cx<float> u = ldg<float>(a.untwist + c + i * C);
+        un[i] = mk<float>(u.x * a.scale, u.y * a.scale); // scale folded in: exact, scale is 2^-m
+    }
+    long long acc_lo[R], acc_hi[R];
+#pragma unroll
+    for (int i = 0; i < R; i++) acc_lo[i] = acc_hi[i] = 0;
+    float err = 0.f;
+#pragma unroll
+    for (int s = 0; s < 2 * K - 1; s++)
+    {
+        const cx<float>* src = a.group + ((long long)s * a.W + p) * M + c;
+        cx<float> x[R];
+#pragma unroll
+        for (int i = 0; i < R; i++) x[i] = __ldcs(src + i * C);
+#pragma unroll
+        for (int st = L0 - 1; st >= 0; st--)
+        {
+            const int h = 1 << (L0 - 1 - st);
+#pragma unroll
+            for (int i = 0; i < R; i++)
+                if (!(i & h)) gs_bfly<float>(x[i], x[i + h], ldg<float>(a.inv_roots + (i >> (L0 - st))));
+        }
+        const int sh = a.w * s;
+#pragma unroll
+        for (int i = 0; i < R; i++)
+        {
+            const cx<float> v = cmul<float>(x[i], un[i]);
+            const float rr = rintf(v.x), ri = rintf(v.y);
+            err = fmaxf(err, group_error(v, rr, ri));
+            acc_lo[i] += (long long)((unsigned long long)(long long)rr << sh);
+            acc_hi[i] += (long long)((unsigned long long)(long long)ri << sh);
+        }
+    }
+    int64_t* dst = a.c + p * 2 * M + c;
+    if (ok)
+    {
+#pragma unroll
+        for (int i = 0; i < R; i++)
+        {
+            const long long j = c + i * C;
+            __stcs(reinterpret_cast<long long*>(dst + i * C), acc_lo[i] + uu_term(a, j, 2 * M));
+            __stcs(reinterpret_cast<long long*>(dst + i * C + M), acc_hi[i] + uu_term(a, j + M, 2 * M));
+        }
+    }
+    report_err(a.max_err, ok ? err : 0.f);
 }
 
 constexpr int SPLIT_SINGLE_MAX_LIMBS = 6; // limb counts compiled for rings N <= 8192
