@@ -29,14 +29,24 @@ template <typename T> __host__ __device__ __forceinline__ cx<T> mk(T r, T i)
 }
 template <typename T> __device__ __forceinline__ cx<T> cadd(cx<T> a, cx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
 template <typename T> __device__ __forceinline__ cx<T> csub(cx<T> a, cx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+// Products with the rounding spelled out (one plain multiply, one fused
+// multiply-add per component) rather than left to the compiler's contraction,
+// which may fuse either product of a*b - c*d and may choose differently in
+// different kernels: every kernel that runs the same butterfly gets the same
+// bits (the batched, per-size, tiled and per-column forms agree exactly).
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 template <typename T> __device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b)
 {
-    return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return mk<T>(rfma(a.x, b.x, -rmul(a.y, b.y)), rfma(a.x, b.y, rmul(a.y, b.x)));
 }
 // a * conj(b)
 template <typename T> __device__ __forceinline__ cx<T> cmulc(cx<T> a, cx<T> b)
 {
-    return mk<T>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+    return mk<T>(rfma(a.x, b.x, rmul(a.y, b.y)), rfma(a.y, b.x, -rmul(a.x, b.y)));
 }
 
 // Radix-2 butterflies, the two units of fft.cuh:69-89.

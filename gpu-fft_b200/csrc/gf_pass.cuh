@@ -381,6 +381,98 @@ __global__ void __launch_bounds__(NTHR, pass_min_blocks<T>()) pass_kernel(const 
 }
 
 // ---------------------------------------------------------------------------
+// Column form of a strided pass of L <= 4 stages. The pass's closed
+// sub-networks are the columns of each stage-s0 group: elements
+// j = g M / 2^s0 + c + i C (i < 2^L, C = M / 2^(s0+L)). One thread owns one
+// column in registers and runs the pass's radix-2 steps with the same
+// twiddles (table[(neg ? 2^s : 0) + (g << u) + (i >> (L-u))] at stage s = s0+u)
+// and in the same order as the tiled kernel, so the values are identical;
+// there is no shared memory and no barrier, neighbouring threads take
+// neighbouring columns (coalesced), and with 2^L elements per thread many
+// more threads are in flight than with 4096-element tiles. Load and store
+// variants are compile-time, so their selection costs nothing per element.
+// ---------------------------------------------------------------------------
+constexpr int COL_MAX_L = 4;
+constexpr int COL_THREADS = 128;
+
+template <typename T, bool FWD, int L, int IK, int OK>
+__global__ void __launch_bounds__(COL_THREADS) col_pass_kernel(const PassArgs<T> a)
+{
+    constexpr int R = 1 << L;
+    const int m = a.geo.m, s0 = a.geo.s0;
+    const int lc = m - s0 - L; // log2 columns per group
+    const long long idx = (long long)blockIdx.x * COL_THREADS + threadIdx.x;
+    const long long b = idx >> (m - L);
+    if (b >= a.batch) return;
+    const long long r = idx & ((1LL << (m - L)) - 1);
+    const long long g = r >> lc;
+    const long long C = 1LL << lc;
+    const long long j0 = (g << (m - s0)) + (r & (C - 1));
+    cx<T> x[R];
+#pragma unroll
+    for (int i = 0; i < R; i++) x[i] = load_elem<T>(a, IK, b, j0 + i * C);
+#pragma unroll
+    for (int k = 0; k < L; k++)
+    {
+        const int u = FWD ? k : L - 1 - k; // stage s0 + u
+        const int h = 1 << (L - 1 - u);
+        const cx<T>* tw = a.table + (a.geo.neg ? (1LL << (s0 + u)) : 0LL) + (g << u);
+#pragma unroll
+        for (int i = 0; i < R; i++)
+        {
+            if (i & h) continue;
+            const cx<T> w = ldg<T>(tw + (i >> (L - u)));
+            if (FWD)
+                ct_bfly<T>(x[i], x[i + h], w);
+            else
+                gs_bfly<T>(x[i], x[i + h], w);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < R; i++) store_elem<T>(a, OK, b, j0 + i * C, x[i]);
+}
+
+// Launch the column form when a kernel for (in_kind, out_kind) is compiled:
+// forward first passes (any load, complex store) and inverse last passes
+// (complex load, any store). Returns -1 when the pair has no column kernel.
+template <typename T, bool FWD, int L>
+static inline int launch_col_pass(const PassArgs<T>& a, cudaStream_t s)
+{
+    const long long threads = a.batch << (a.geo.m - L);
+    const unsigned blocks = (unsigned)((threads + COL_THREADS - 1) / COL_THREADS);
+    auto go = [&](auto kern) {
+        kern<<<blocks, COL_THREADS, 0, s>>>(a);
+        return check_launch();
+    };
+    if constexpr (FWD)
+    {
+        if (a.out_kind != OUT_CPX) return -1;
+        switch (a.in_kind)
+        {
+        case IN_CPX: return go(col_pass_kernel<T, true, L, IN_CPX, OUT_CPX>);
+        case IN_REAL: return go(col_pass_kernel<T, true, L, IN_REAL, OUT_CPX>);
+        case IN_FOLD: return go(col_pass_kernel<T, true, L, IN_FOLD, OUT_CPX>);
+        case IN_FOLD2: return go(col_pass_kernel<T, true, L, IN_FOLD2, OUT_CPX>);
+        case IN_LIN2: return go(col_pass_kernel<T, true, L, IN_LIN2, OUT_CPX>);
+        case IN_VJP3: return go(col_pass_kernel<T, true, L, IN_VJP3, OUT_CPX>);
+        default: return -1;
+        }
+    }
+    else
+    {
+        if (a.in_kind != IN_CPX) return -1;
+        switch (a.out_kind)
+        {
+        case OUT_CPX: return go(col_pass_kernel<T, false, L, IN_CPX, OUT_CPX>);
+        case OUT_REAL: return go(col_pass_kernel<T, false, L, IN_CPX, OUT_REAL>);
+        case OUT_UNFOLD: return go(col_pass_kernel<T, false, L, IN_CPX, OUT_UNFOLD>);
+        case OUT_RE2: return go(col_pass_kernel<T, false, L, IN_CPX, OUT_RE2>);
+        default: return -1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 struct Plan
@@ -449,6 +541,11 @@ static inline int launch_pass(const PassArgs<T>& a, const Plan& p, int k, long l
     const int L = p.L[k];
     if (k == p.np - 1)
         return dispatch_int<1, EBITS>(L, [&]<int LL>() { return launch_pass_shape<T, FWD, LL, false>(a, ctas, s); });
+    if (L <= COL_MAX_L)
+    {
+        const int st = dispatch_int<1, COL_MAX_L>(L, [&]<int LL>() { return launch_col_pass<T, FWD, LL>(a, s); });
+        if (st >= 0) return st;
+    }
     return dispatch_int<1, 9>(L, [&]<int LL>() { return launch_pass_shape<T, FWD, LL, true>(a, ctas, s); });
 }
 
