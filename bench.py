@@ -30,7 +30,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SEED = 20261203 + 3  # config 3 of the workload list
+SEED = 20261203 + 3  # seed of the N = 2^16, batch 256 product workload
 
 
 def parse():
@@ -40,9 +40,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64", "batch", "vjp"], default="split",
-                   help="split/f64/f32/dropin_f64: config 3 (N = 2^16 negacyclic products); "
-                        "batch: config 4 (4096 mixed ring sizes 2^10..2^17, one persistent launch in a CUDA "
-                        "graph); vjp: config 5 (FP32 linear convolution N = 2^14, batch 512, forward + VJP)")
+                   help="split/f64/f32/dropin_f64: N = 2^16 negacyclic products, batch 256, 24-bit coefficients; "
+                        "batch: 4096 mixed ring sizes 2^10..2^17 (one persistent launch in a CUDA "
+                        "graph); vjp: FP32 linear convolution N = 2^14, batch 512, forward + VJP")
     p.add_argument("--no-compare", dest="compare", action="store_false",
                    help="time only --path (by default FP64 is timed beside it)")
     p.add_argument("--n-power", type=int, default=16)
@@ -291,8 +291,55 @@ def time_path(step, host_step, a, b, c, hosts, args, stream, torch, barrier, max
     return ms, ms_e2e, t0, t1
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dominant kernels, from one ncu capture each of the workload named in the
+# profile summary; a wave of these sizes moves the same bytes per launch.
+NCU_TRAFFIC = {
+    "pass_kernel<f32,fwd,L12,contiguous>": (64.88e6, "profiles/pass_kernel_f32_L12_split_N65536.md"),
+    "fused_kernel<f64,L12,middle>": (39.38e6, "profiles/fused_kernel_f64_L12_N65536.md"),
+}
+
+
+def traced_kernels(gf, step, a, b, c, args, stream, torch, barrier, max_over_ranks):
+    """Re-run the K timed steps with the library's per-kernel event tracing on:
+    (per-kernel rows longest first, ms per step of the traced run)."""
+    barrier()
+    gf.trace_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(a, b, c)
+    e1.record(stream)
+    barrier()
+    gf.trace_enable(False)
+    rows = gf.trace_collect()
+    return rows, max_over_ranks(e0.elapsed_time(e1) / args.steps)
+
+
+def kernel_roofline(rows, peak, peak_kind, ms_traced, steps):
+    """Roofline of the dominant kernel (largest summed device time): its
+    algorithmic bytes per launch over its mean CUDA-event launch duration."""
+    dom = rows[0]
+    per_launch_ms = dom["ms"] / dom["launches"]
+    per_launch_bytes = dom["alg_bytes"] / dom["launches"]
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    total = sum(r["ms"] for r in rows)
+    traffic = NCU_TRAFFIC.get(dom["kernel"])
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "traffic": traffic[0] if traffic else None,
+            "traffic_source": traffic[1] if traffic else None,
+            "kernel": dom["kernel"], "launches_per_step": dom["launches"] / steps,
+            "mean_launch_us": per_launch_ms * 1e3, "alg_bytes_per_launch": per_launch_bytes,
+            "share_of_step": dom["ms"] / total if total else None,
+            "timed": "CUDA events around each launch (library tracing) over a repeat of the timed steps",
+            "traced_ms_per_step": ms_traced,
+            "kernels": [{"kernel": r["kernel"], "launches_per_step": r["launches"] / steps,
+                         "ms_per_step": r["ms"] / steps,
+                         "gbs": (r["alg_bytes"] / (r["ms"] * 1e-3) / 1e9) if r["ms"] else None} for r in rows]}
+
+
 def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, peak, peak_kind):
-    """Config 4: 4096 negacyclic products, ring sizes log-uniform over 2^10..2^17,
+    """Mixed sizes: 4096 negacyclic products, ring sizes log-uniform over 2^10..2^17,
     coefficients in [-2^15, 2^15), FP64, one persistent launch replayed from a
     CUDA graph; per-size sequential launches timed beside it."""
     import numpy as np
@@ -371,6 +418,9 @@ def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cl
         e5.record(s)
         barrier()
         ms_e2e = max_over_ranks(e4.elapsed_time(e5) / args.steps)
+        # the persistent kernel timed per launch (direct launches: graph replays are not traced)
+        rows, ms_traced = traced_kernels(gf, lambda x, y, z: plan.execute(x, y, z, stream=s), a, b, c, args, s,
+                                         torch, barrier, max_over_ranks)
     alg = 3 * plan.total * 8
     achieved = alg / (ms * 1e-3) / 1e9
     info = plan.info()
@@ -382,21 +432,21 @@ def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cl
         "config": {"workload": "4096 negacyclic products, ring sizes log-uniform 2^10..2^17, FP64, one persistent "
                                "cooperative launch replayed from a CUDA graph", "requests": 4096,
                    "coefficients": plan.total, "launch_shape": info, "l2": "inputs larger than L2 (no flush)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_step": alg,
-                     "timed": "graph replay of the persistent launch, CUDA events"},
+        "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps),
+        "chain": {"achieved_gbs": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": alg,
+                  "timed": "graph replay of the persistent launch, CUDA events"},
         "e2e": {"value": world * 4096 / (ms_e2e * 1e-3), "unit": "products/s", "h2d_bytes_per_step": 2 * alg // 3,
                 "d2h_bytes_per_step": alg // 3},
         "per_size_sequential": {"value": world * 4096 / (ms_seq * 1e-3), "unit": "products/s", "ms_per_step": ms_seq,
                                 "identical_outputs": identical},
-        "gpu_launches": args.steps, "clocks": clk.summary(t0, t1),
+        "gpu_launches": sum(r["launches"] for r in rows), "clocks": clk.summary(t0, t1),
     }
     plan.close()
     return line
 
 
 def run_vjp(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, peak, peak_kind):
-    """Config 5: FP32 linear convolution N = 2^14 (zero-padded to 2^15), batch
+    """Convolution training step: FP32 linear convolution N = 2^14 (zero-padded to 2^15), batch
     512; a step is the forward product plus the VJP for both operands."""
     n, batch = 1 << 14, 512
     g = torch.Generator().manual_seed(SEED + 2 + rank)
@@ -448,6 +498,8 @@ def run_vjp(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls,
     e3.record(stream)
     barrier()
     ms_e2e = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+    rows, ms_traced = traced_kernels(gf, lambda x, y, z: step(), a, b, c, args, stream, torch, barrier,
+                                     max_over_ranks)
     # forward: a, b in (2N*4 bytes), c out (2N*4); backward: g (2N*4), a, b in, grads out (2N*4)
     alg = batch * (4 * n * 4 + 6 * n * 4)
     achieved = alg / (ms * 1e-3) / 1e9
@@ -458,12 +510,12 @@ def run_vjp(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls,
         "dtype": "f32", "data": "synthetic (seeded i.i.d. N(0,1))",
         "config": {"workload": "real FP32 linear convolution N=2^14 zero-padded to 2^15, batch 512, forward + VJP",
                    "batch_per_gpu": batch, "l2": "inputs larger than L2 (no flush)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_step": alg,
-                     "timed": "forward product + VJP per step, CUDA events"},
+        "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps),
+        "chain": {"achieved_gbs": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": alg,
+                  "timed": "forward product + VJP per step, CUDA events"},
         "e2e": {"value": world * batch / (ms_e2e * 1e-3), "unit": "products/s",
                 "h2d_bytes_per_step": batch * 4 * n * 4, "d2h_bytes_per_step": batch * 4 * n * 4},
-        "gpu_launches": 6 * args.steps, "clocks": clk.summary(t0, t1),
+        "gpu_launches": sum(r["launches"] for r in rows), "clocks": clk.summary(t0, t1),
     }
 
 
@@ -523,8 +575,11 @@ def main():
             c = torch.empty((batch, n), dtype=dout, device=dev)
             ms, ms_e2e, t0, t1 = time_path(step, host_step, a, b, c, (a_host, b_host, c_host), args, stream, torch,
                                            barrier, max_over_ranks)
+            rows, ms_traced = traced_kernels(gf, step, a, b, c, args, stream, torch, barrier, max_over_ranks)
             achieved = alg * batch / (ms * 1e-3) / 1e9
             results[name] = dict(ms=ms, ms_e2e=ms_e2e, t0=t0, t1=t1, alg=alg, launches=launches,
+                                 kroof=kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps),
+                                 traced_launches=sum(r["launches"] for r in rows),
                                  value=world * batch / (ms * 1e-3), achieved=achieved,
                                  h2d=2 * batch * n * a_host.element_size(), d2h=batch * n * c_host.element_size(),
                                  dtype={torch.float64: "f64", torch.float32: "f32", torch.int32: "f32"}[din],
@@ -543,13 +598,13 @@ def main():
                                f"coefficients in [0, 2^24), path {args.path}",
                    "ring_log2": n_power, "batch_per_gpu": batch, "path": args.path,
                    "l2": "inputs larger than L2 (no flush)"},
-        "roofline": {"bound": "hbm", "achieved": main_r["achieved"], "peak": peak, "unit": "GB/s",
-                     "frac": main_r["achieved"] / peak, "peak_kind": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_product": main_r["alg"],
-                     "timed": "whole product chain (all launches of one step), CUDA events"},
+        "roofline": main_r["kroof"],
+        "chain": {"achieved_gbs": main_r["achieved"], "frac": main_r["achieved"] / peak,
+                  "algorithmic_bytes_per_product": main_r["alg"],
+                  "timed": "whole product chain (all launches of one step), CUDA events"},
         "e2e": {"value": world * batch / (main_r["ms_e2e"] * 1e-3), "unit": "products/s",
                 "h2d_bytes_per_step": main_r["h2d"], "d2h_bytes_per_step": main_r["d2h"]},
-        "gpu_launches": main_r["launches"] * args.steps,
+        "gpu_launches": main_r["traced_launches"],
         "clocks": clk.summary(t_lo, t_hi),
     }
     for name, r in results.items():
@@ -557,6 +612,8 @@ def main():
             continue
         line[name] = {"value": r["value"], "unit": "products/s", "ms_per_step": r["ms"],
                       "roofline_frac": r["achieved"] / peak, "achieved_gbs": r["achieved"],
+                      "dominant_kernel": {k: r["kroof"][k] for k in ("kernel", "achieved", "frac", "mean_launch_us",
+                                                                     "share_of_step", "traffic")},
                       "e2e_value": world * batch / (r["ms_e2e"] * 1e-3)}
     if rank == 0:
         # exactness spot check of the first product: 64 sampled coefficients

@@ -108,6 +108,9 @@ def lib() -> ctypes.CDLL:
         L.gpufft_negacyclic_mul_split_workspace_bytes.argtypes = [i, i, i]
         L.gpufft_negacyclic_mul_split_workspace_bytes.restype = sz
         L.gpufft_negacyclic_mul_split_f32.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, vp, sz, vp, vp]
+        L.gpufft_trace_enable.argtypes = [i]
+        L.gpufft_trace_collect.argtypes = [i, ctypes.c_char_p, i, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ll), ctypes.POINTER(i)]
         L.gpufft_negacyclic_mul_host_workspace_bytes.argtypes = [i, i, i, i]
         L.gpufft_negacyclic_mul_host_workspace_bytes.restype = sz
         L.gpufft_negacyclic_mul_f32_host.argtypes = [vp, vp, vp, i, i, i, vp, vp, sz, vp]
@@ -320,6 +323,31 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
         _stream_handle(stream))
     check(st, "negacyclic_mul_split")
     return (out, err) if return_error else out
+
+
+# ---------------------------------------------------------------------------
+# Per-kernel device-time tracing
+# ---------------------------------------------------------------------------
+def trace_enable(on: bool = True) -> None:
+    """Bracket every library kernel launch with CUDA events (off by default)."""
+    check(lib().gpufft_trace_enable(int(bool(on))), "trace_enable")
+
+
+def trace_collect(max_rows: int = 64):
+    """Per-kernel totals recorded since the last collect, longest first:
+    [{"kernel", "ms", "launches", "alg_bytes"}]. Waits for the recorded events."""
+    name_len = 112
+    names = ctypes.create_string_buffer(max_rows * name_len)
+    ms = (ctypes.c_double * max_rows)()
+    by = (ctypes.c_double * max_rows)()
+    n = (ctypes.c_longlong * max_rows)()
+    rows = ctypes.c_int()
+    check(lib().gpufft_trace_collect(max_rows, names, name_len, ms, by, n, ctypes.byref(rows)), "trace_collect")
+    out = []
+    for k in range(rows.value):
+        nm = names.raw[k * name_len:(k + 1) * name_len].split(b"\0", 1)[0].decode()
+        out.append({"kernel": nm, "ms": ms[k], "launches": int(n[k]), "alg_bytes": by[k]})
+    return sorted(out, key=lambda r: -r["ms"])
 
 
 def _host_operands(a, b, dtypes, what):

@@ -29,6 +29,8 @@
 // kept, cached in a JSON file keyed by GPU name, driver version and precision.
 #include "gf_fused.cuh"
 
+#include <cmath>
+
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -290,6 +292,10 @@ template <typename T, int MINB> static int batch_launch(BatchPlan* P, const void
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    double coeffs = 0;
+    for (int np : P->n_powers) coeffs += std::ldexp(1.0, np);
+    // a and b read, c written once each
+    GF_TRACE(tr, 3.0 * coeffs * sizeof(T), s, "batch_kernel<%s,%d CTA/SM>", sizeof(T) == 4 ? "f32" : "f64", MINB);
     e = cudaLaunchKernelEx(&cfg, batch_kernel<T, MINB>, A);
     if (e != cudaSuccess) return set_cuda_error(e);
     return check_launch();

@@ -1,11 +1,12 @@
 // gpufft-b200: shared device/host helpers for the sm_100a kernels.
 //
 // Complex values use the reference's COMPLEX<T> layout (complex.cuh:28-34):
-// a float2 / double2 with the real part first. The arithmetic below keeps the
-// reference's expression shapes (complex.cuh:65-69 add, 99-104 sub, 133-139
-// mul) so that the compiler contracts them to FMA the same way it does for
-// the reference kernels.
+// a float2 / double2 with the real part first. The arithmetic below computes
+// the reference's expressions (complex.cuh:65-69 add, 99-104 sub, 133-139 mul)
+// with the multiply-add rounding fixed explicitly (see cmul).
 #pragma once
+
+#include <cstdio>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -80,6 +81,37 @@ namespace gfb
 {
 int set_cuda_error(cudaError_t e);
 int check_launch();
+
+// Per-kernel device-time tracing (gpufft_trace_enable / gpufft_trace_collect).
+// While tracing is on, every kernel launch of the product paths is bracketed
+// by two CUDA events on its stream and tagged with its name and the
+// algorithmic bytes it must move (inputs read once plus outputs written once);
+// collecting sums elapsed time and bytes per kernel name. Off, a scope costs
+// one relaxed atomic load.
+bool trace_on();
+void* trace_begin(const char* name, double alg_bytes, cudaStream_t s);
+void trace_end(void* rec, cudaStream_t s);
+struct TraceScope
+{
+    void* rec = nullptr;
+    cudaStream_t s;
+    TraceScope(const char* name, double alg_bytes, cudaStream_t st) : s(st)
+    {
+        if (trace_on()) rec = trace_begin(name, alg_bytes, st);
+    }
+    ~TraceScope()
+    {
+        if (rec) trace_end(rec, s);
+    }
+    TraceScope(const TraceScope&) = delete;
+    TraceScope& operator=(const TraceScope&) = delete;
+};
+// Declares `var`, a TraceScope named by the printf-style arguments (formatted
+// only while tracing is on).
+#define GF_TRACE(var, bytes, stream, ...)                                                                              \
+    char var##_name[112] = {0};                                                                                        \
+    if (::gfb::trace_on()) snprintf(var##_name, sizeof(var##_name), __VA_ARGS__);                                      \
+    ::gfb::TraceScope var(var##_name, (double)(bytes), stream)
 
 // Number of SMs of the current device (cached per device ordinal).
 inline int sm_count()

@@ -119,6 +119,9 @@ template <int L, bool SINGLE> static int launch_vjp_shape(const VjpArgs& a, long
     static int done[64] = {0};
     int st = ensure_smem(vjp_kernel<L, SINGLE>, smem, done);
     if (st) return st;
+    // three spectra (G, A, B) in, two gradients out, per point of the half-length transform
+    GF_TRACE(tr, (double)a.batch * (double)(1LL << a.geo.m) * 5 * sizeof(cx<float>), s, "vjp_kernel<L%d,%s>", L,
+             SINGLE ? "single" : "middle");
     vjp_kernel<L, SINGLE><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
     return check_launch();
 }

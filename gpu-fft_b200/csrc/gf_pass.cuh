@@ -380,6 +380,27 @@ __global__ void __launch_bounds__(NTHR, pass_min_blocks<T>()) pass_kernel(const 
     pass_body<T, FWD, L, STRIDED>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
 }
 
+// Algorithmic bytes of one pass launch: every element of the pass read once in
+// its load variant's format and written once in its store variant's format.
+template <typename T> inline double pass_alg_bytes(const PassArgs<T>& a)
+{
+    const double E = (double)a.batch * (double)(1LL << a.geo.m), t = sizeof(T), c = 2 * sizeof(T);
+    double in = c, out = c;
+    switch (a.in_kind)
+    {
+    case IN_REAL: in = a.zero_pad ? t / 2 : t; break;
+    case IN_LIN2: in = t; break;
+    case IN_VJP3: in = 4 * t / 3; break;
+    case IN_PROD: in = 2 * c; break;
+    case IN_GROUP: in = 2 * a.gk * c; break;
+    case IN_CPX: in = a.zero_pad ? c / 2 : c; break;
+    default: break;
+    }
+    if (a.out_kind == OUT_REAL || a.out_kind == OUT_RE2) out = t;
+    return E * (in + out);
+}
+inline const char* kind_name(int fwd) { return fwd ? "fwd" : "inv"; }
+
 // ---------------------------------------------------------------------------
 // Column form of a strided pass of L <= 4 stages. The pass's closed
 // sub-networks are the columns of each stage-s0 group: elements
@@ -441,6 +462,8 @@ static inline int launch_col_pass(const PassArgs<T>& a, cudaStream_t s)
     const long long threads = a.batch << (a.geo.m - L);
     const unsigned blocks = (unsigned)((threads + COL_THREADS - 1) / COL_THREADS);
     auto go = [&](auto kern) {
+        GF_TRACE(tr, pass_alg_bytes(a), s, "col_pass<%s,%s,L%d,in%d,out%d>", sizeof(T) == 4 ? "f32" : "f64",
+                 kind_name(FWD), L, a.in_kind, a.out_kind);
         kern<<<blocks, COL_THREADS, 0, s>>>(a);
         return check_launch();
     };
@@ -528,6 +551,8 @@ static inline int launch_pass_shape(const PassArgs<T>& a, long long ctas, cudaSt
     static int smem_done[64] = {0};
     int st = ensure_smem(pass_kernel<T, FWD, L, STRIDED>, smem, smem_done);
     if (st) return st;
+    GF_TRACE(tr, pass_alg_bytes(a), s, "pass_kernel<%s,%s,L%d,%s>", sizeof(T) == 4 ? "f32" : "f64",
+             kind_name(FWD), L, STRIDED ? "strided" : "contiguous");
     pass_kernel<T, FWD, L, STRIDED><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
     return check_launch();
 }

@@ -68,9 +68,12 @@ static bool choose_limbs(int n_power, int input_bits, bool non_negative, int* w_
 static long long split_wave(int m, int k, long long batch)
 {
     const size_t per = (size_t)(4 * k - 1) * ((size_t)1 << m) * sizeof(cx<float>);
-    // waves of up to 112 MiB of limb and group spectra (resident in the 126 MB
-    // L2), rounded so that the contiguous passes fill whole waves of the SMs
-    long long w = (long long)((112ull << 20) / per);
+    // Recommended wave: up to 1.25 GiB of limb and group spectra, rounded so
+    // that the contiguous passes fill whole waves of the SMs. Measured at
+    // N = 2^16 (k = 5, 4.75 MiB per product), batch 256: waves of 23 / 74 / 256
+    // products run 161k / 183k / 198k products/s -- CTAs per launch matter more
+    // than keeping a wave inside the 126 MB L2.
+    long long w = (long long)((1280ull << 20) / per);
     if (m > EBITS) w = round_wave(w, ((long long)1 << m) / ECTA);
     if (w < 1) w = 1;
     return w < batch ? w : batch;
@@ -137,10 +140,15 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         A.voff = hoff - A.K;
     }
 
-    long long W = split_wave(m, k, batch);
+    // the workspace sets the wave (as many products as it holds, rounded to
+    // whole waves of the SMs for the tiled passes)
     const size_t need1 = split_ws_bytes(m, k, 1);
     if (!ws || ws_bytes < need1) return GPUFFT_ERROR_WORKSPACE;
-    if (split_ws_bytes(m, k, W) > ws_bytes) W = (long long)(ws_bytes / need1);
+    long long W = (long long)(ws_bytes / need1);
+    if (W >= batch)
+        W = batch;
+    else if (m > EBITS)
+        W = round_wave(W, M / ECTA);
     if (max_err && reset_err)
     {
         cudaError_t e = cudaMemsetAsync(max_err, 0, sizeof(unsigned), s);
@@ -177,6 +185,8 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         {
             const long long threads = 2 * wv * k * (M >> L0);
             const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
+            // int32 rows of both operands in, 2k limb spectra out
+            GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * 8), s, "split_fwd0_col<L%d,k%d>", L0, k);
             st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
                 split_fwd0_col<LL><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
                 return check_launch();
@@ -204,10 +214,14 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         //    (2k-1) W groups in place
         {
             const long long pts = wv * M;
-            st = dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
-                split_groups<KK><<<(unsigned)((pts + 255) / 256), 256, 0, s>>>(A);
-                return check_launch();
-            });
+            {
+                // 2k limb spectra in, 2k-1 group spectra out
+                GF_TRACE(tr, (double)pts * 8 * (4 * k - 1), s, "split_groups<k%d>", k);
+                st = dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
+                    split_groups<KK><<<(unsigned)((pts + 255) / 256), 256, 0, s>>>(A);
+                    return check_launch();
+                });
+            }
             if (st) return st;
             PassArgs<float> q{};
             q.geo = pass_geo(p, 1, m, 0, (2 * k - 1) * wv, &ctas);
@@ -226,6 +240,8 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         {
             const long long threads = wv * (M >> L0);
             const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
+            // 2k-1 group spectra in, int64 rows out
+            GF_TRACE(tr, (double)wv * M * ((2 * k - 1) * 8 + 2 * 8), s, "split_inv0_col<L%d,k%d>", L0, k);
             st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
                 return dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
                     split_inv0_col<LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);

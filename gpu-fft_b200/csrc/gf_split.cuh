@@ -17,14 +17,17 @@
 // of any C_s value to its nearest integer ("pre-rounding error") is measured
 // on the device and returned, so exactness (error < 0.5) is checked per call.
 //
-// Kernels (N > 8192, per wave of products; workspace in L2):
-//   split_fwd0   strided first forward pass for the 2k limb polynomials of a
-//                product column block: the int32 inputs are loaded once, each
-//                limb is extracted, folded, twisted and transformed in turn;
-//   split_mid    contiguous last forward pass of all 2k limb spectra, the
-//                2k-1 pointwise group sums and the first inverse pass of each;
-//   split_inv0   strided last inverse pass of every group with scale, untwist,
-//                unfold, rounding and the int64 recombination in registers.
+// Kernels (N > 8192, per wave of products; the workspace size sets the wave):
+//   split_fwd0_col / split_fwd0   first forward pass (strided) of the 2k limb
+//                polynomials: limb digit extraction, fold and twist in the load
+//                (one thread per column when the pass has <= 4 stages, 4096-
+//                element tiles otherwise);
+//   pass_kernel  contiguous last forward pass of all 2k limb spectra;
+//   split_groups the 2k-1 pointwise limb-group sums (plus the centring term);
+//   pass_kernel  contiguous first inverse pass of every group;
+//   split_inv0_col / split_inv0   last inverse pass (strided) of every group
+//                with scale, untwist, unfold, rounding and the int64
+//                recombination in registers.
 // N <= 8192 runs all of it in one kernel (split_mid<true>).
 #pragma once
 
@@ -529,6 +532,10 @@ template <typename K> static int launch_split(K* kern, int* done, const SplitArg
     const size_t smem = sizeof(cx<float>) * SMEM_ELEMS;
     int st = ensure_smem(kern, smem, done);
     if (st) return st;
+    // tiled split kernels: int32 inputs of W products in, int64 outputs, and
+    // the spectra of the chain's other side (upper estimate)
+    const double M = (double)(1LL << a.geo.m);
+    GF_TRACE(tr, (double)a.W * M * (2 * 2 * 4 + 2 * 8 + (4 * a.k - 1) * 8), s, "split_tiled<k%d>", a.k);
     kern<<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
     return check_launch();
 }

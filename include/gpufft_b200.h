@@ -52,6 +52,17 @@ enum { GPUFFT_FORWARD = 0, GPUFFT_INVERSE = 1 };
 /* gpufft::ReductionPolynomial (reference fft_cpu.cuh:69-73) */
 enum { GPUFFT_X_N_PLUS = 0, GPUFFT_X_N_MINUS = 1 };
 
+/* Per-kernel device-time tracing (no reference counterpart). While enabled,
+ * each kernel launch of the library's entry points (outside stream capture)
+ * is bracketed by two CUDA events on its stream and tagged with the kernel's
+ * name and the algorithmic bytes it moves (inputs read once, outputs written
+ * once). gpufft_trace_collect waits for the recorded events, returns up to
+ * max_rows per-kernel totals (names NUL-terminated in slots of name_len bytes,
+ * summed milliseconds, summed bytes, launch counts) and clears the records. */
+int gpufft_trace_enable(int on);
+int gpufft_trace_collect(int max_rows, char* names, int name_len, double* total_ms, double* alg_bytes,
+                         long long* launches, int* rows);
+
 /* The cudaError_t of the last GPUFFT_ERROR_CUDA raised on this host thread. */
 int gpufft_last_cuda_error(void);
 /* A static, human-readable string for a gpufft_status value. */

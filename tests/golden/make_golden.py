@@ -10,7 +10,7 @@ Each .npz holds seeded inputs and the reference's outputs for them:
 * ffnt_tables_{f64,f32}.npz  FFNT<T>(4096) root / inverse-root / twist / untwist tables
 * cpu_fft_f64.npz            FFT<double>(1024).fft and .ifft of a seeded complex vector
 * ffnt_mult_f64.npz          FFNT<double>(4096).MULT of seeded inputs in [0, 2^12)
-* linear_f64.npz             config-1 product: N = 2^12, coefficients in [-2^15, 2^15),
+* linear_f64.npz             CPU-example product: N = 2^12, coefficients in [-2^15, 2^15),
                              FFT<double>(4096) fft/fft/product/ifft/round as in the
                              reference's CPU example (example/test_fft_cpu.cu)
 * schoolbook_q7.npz          schoolbook_poly_multiplication (negacyclic, mod 7) and

@@ -89,3 +89,9 @@ def test_split_plan_host_logic(gf):
     w, k = gf.split_plan(12, 24, True)
     assert w * k >= 24 and k <= 4
     assert gf.split_plan(16, 16, False)[0] * gf.split_plan(16, 16, False)[1] >= 16
+
+
+def test_trace_collect_without_records(gf):
+    # tracing is off by default; collecting with nothing recorded needs no GPU
+    gf.trace_enable(False)
+    assert gf.trace_collect() == []

@@ -1,4 +1,4 @@
-"""GPU tests of the mixed-size batch plan (config 4 of the workload list):
+"""GPU tests of the mixed-size batch plan (4096 requests, ring sizes 2^10..2^17):
 requests with ring sizes 2^10 .. 2^17 run in one persistent cooperative launch
 (captured in a CUDA graph) and must give outputs identical to per-size
 sequential launches of gpufft_negacyclic_mul_*; FP64 results of 16-bit
@@ -58,8 +58,8 @@ def test_batch_matches_per_size_launches(gf, O, dev, dtype):
     plan.close()
 
 
-def test_batch_config4_graph_and_autotune(gf, dev):
-    # config 4: 4096 requests, ring sizes log-uniform over 2^10..2^17, FP64,
+def test_batch_4096_mixed_sizes_graph_and_autotune(gf, dev):
+    # the full mixed workload: 4096 requests, ring sizes log-uniform over 2^10..2^17, FP64,
     # one persistent launch captured in a CUDA graph, autotuned launch shape
     rng = np.random.default_rng(4)
     n_powers = make_requests(rng, 4096)

@@ -67,8 +67,8 @@ def test_vjp_vs_direct_correlation(gf, dev, n_power, batch):
     assert rel(gb.cpu().numpy(), wb) < 2e-5
 
 
-def test_vjp_config5_finite_differences(gf, dev):
-    # config 5: N = 2^14 (padded to 2^15), batch 512, a, b, g i.i.d. N(0,1); the VJP
+def test_vjp_n16384_batch512_finite_differences(gf, dev):
+    # the convolution workload: N = 2^14 (padded to 2^15), batch 512, a, b, g i.i.d. N(0,1); the VJP
     # of L = <g, a*b> against FP64 central differences along 64 random directions
     rng = np.random.default_rng(5)
     n, batch = 1 << 14, 512

@@ -130,8 +130,8 @@ def test_r2r_linear_product(gf, O, dev, T, n_power, zero_padding):
         assert np.array_equal(np.rint(got[k * M:(k + 1) * M]).astype(np.int64), exact)
 
 
-def test_config1_linear_product_bit_exact_vs_reference(gf, O, dev):
-    # config 1: R_R product, N = 2^12, batch 1, FP64, coefficients in [-2^15, 2^15)
+def test_cpu_example_linear_product_bit_exact_vs_reference(gf, O, dev):
+    # the CPU-example product: R_R, N = 2^12, batch 1, FP64, coefficients in [-2^15, 2^15)
     g = np.load(os.path.join(GOLD, "linear_f64.npz"))
     n = int(g["n"])
     M = 2 * n

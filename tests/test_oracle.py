@@ -49,8 +49,8 @@ def test_ffnt_mult_matches_golden_and_schoolbook(O):
     assert np.array_equal(out.view(np.int64), exact)
 
 
-def test_linear_config1_golden_is_exact(O):
-    # config 1: N = 2^12, coefficients in [-2^15, 2^15): the reference's FFT<double>
+def test_linear_cpu_example_golden_is_exact(O):
+    # the CPU-example product: N = 2^12, coefficients in [-2^15, 2^15): the reference's FFT<double>
     # product rounds to the exact schoolbook product.
     g = load("linear_f64.npz")
     exact = O.wrap64(O.schoolbook(g["a"], g["b"], O.LINEAR))

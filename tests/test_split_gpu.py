@@ -38,8 +38,8 @@ def test_split_exact(gf, O, dev, n_power, batch, lo, hi):
         assert np.array_equal(got[:, idx], exact_rows(O, a, b, idx))
 
 
-def test_split_config3_full_batch(gf, O, dev):
-    # config 3 at N = 2^16, batch 256, coefficients uniform in [0, 2^24): exact on
+def test_split_n65536_batch256(gf, O, dev):
+    # the headline workload: N = 2^16, batch 256, coefficients uniform in [0, 2^24): exact on
     # sampled coefficients of sampled products; error report below 0.5
     rng = np.random.default_rng(3)
     n, batch = 1 << 16, 256
