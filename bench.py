@@ -291,12 +291,17 @@ def time_path(step, host_step, a, b, c, hosts, args, stream, torch, barrier, max
     return ms, ms_e2e, t0, t1
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# dominant kernels, from one ncu capture each of the workload named in the
-# profile summary; a wave of these sizes moves the same bytes per launch.
+# DRAM traffic of the dominant kernels as a fraction of their algorithmic
+# bytes, from one ncu capture each of a smaller wave of the same kernel
+# (dram__bytes_read.sum + dram__bytes_write.sum over the kernel's algorithmic
+# bytes; ncu flushes caches before each replay, so this is the cold-cache
+# figure). Both scale with the products per launch, so traffic per launch =
+# ratio x measured algorithmic bytes per launch.
 NCU_TRAFFIC = {
-    "pass_kernel<f32,fwd,L12,contiguous>": (64.88e6, "profiles/pass_kernel_f32_L12_split_N65536.md"),
-    "fused_kernel<f64,L12,middle>": (39.38e6, "profiles/fused_kernel_f64_L12_N65536.md"),
+    # wave of 46 products (3680 CTAs): 120.8 MB read + 61.8 MB written / 241.2 MB
+    "pass_kernel<f32,fwd,L12,contiguous>": (182.6 / 241.2, "profiles/pass_kernel_f32_L12_split_N65536.md"),
+    # wave of 74 products (592 CTAs): 78.2 MB read + 2.8 MB written / 116.4 MB
+    "fused_kernel<f64,L12,middle>": (81.0 / 116.4, "profiles/fused_kernel_f64_L12_N65536.md"),
 }
 
 
@@ -326,8 +331,9 @@ def kernel_roofline(rows, peak, peak_kind, ms_traced, steps):
     total = sum(r["ms"] for r in rows)
     traffic = NCU_TRAFFIC.get(dom["kernel"])
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_kind": peak_kind, "traffic": traffic[0] if traffic else None,
-            "traffic_source": traffic[1] if traffic else None,
+            "peak_kind": peak_kind, "traffic": traffic[0] * per_launch_bytes if traffic else None,
+            "traffic_source": (traffic[1] + " (cold-cache ncu capture of a smaller wave, scaled by products "
+                               "per launch)") if traffic else None,
             "kernel": dom["kernel"], "launches_per_step": dom["launches"] / steps,
             "mean_launch_us": per_launch_ms * 1e3, "alg_bytes_per_launch": per_launch_bytes,
             "share_of_step": dom["ms"] / total if total else None,
