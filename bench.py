@@ -39,10 +39,11 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64", "batch", "vjp"], default="split",
+    p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64", "batch", "vjp", "cc"], default="split",
                    help="split/f64/f32/dropin_f64: N = 2^16 negacyclic products, batch 256, 24-bit coefficients; "
                         "batch: 4096 mixed ring sizes 2^10..2^17 (one persistent launch in a CUDA "
-                        "graph); vjp: FP32 linear convolution N = 2^14, batch 512, forward + VJP")
+                        "graph); vjp: FP32 linear convolution N = 2^14, batch 512, forward + VJP; cc: C_C cyclic "
+                        "products through GPU_FFT, FP32 and FP64, N = 2^10..2^16, ~1 GiB batches")
     p.add_argument("--no-compare", dest="compare", action="store_false",
                    help="time only --path (by default FP64 is timed beside it)")
     p.add_argument("--n-power", type=int, default=16)
@@ -427,6 +428,7 @@ def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cl
         # the persistent kernel timed per launch (direct launches: graph replays are not traced)
         rows, ms_traced = traced_kernels(gf, lambda x, y, z: plan.execute(x, y, z, stream=s), a, b, c, args, s,
                                          torch, barrier, max_over_ranks)
+        split_line = run_batch_split(args, gf, dev, torch, n_powers, a, b, s, barrier, max_over_ranks, world)
     alg = 3 * plan.total * 8
     achieved = alg / (ms * 1e-3) / 1e9
     info = plan.info()
@@ -445,8 +447,60 @@ def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cl
                 "d2h_bytes_per_step": alg // 3},
         "per_size_sequential": {"value": world * 4096 / (ms_seq * 1e-3), "unit": "products/s", "ms_per_step": ms_seq,
                                 "identical_outputs": identical},
+        "split": split_line,
         "gpu_launches": sum(r["launches"] for r in rows), "clocks": clk.summary(t0, t1),
     }
+    plan.close()
+    return line
+
+
+def run_batch_split(args, gf, dev, torch, n_powers, a64, b64, s, barrier, max_over_ranks, world):
+    """The same 4096 mixed-size requests, exact: FP32 split products per size
+    class replayed from one CUDA graph, and per-size split calls beside it."""
+    plan = gf.SplitBatchPlan(n_powers, input_bits=16, non_negative=False)
+    a, b = a64.to(torch.int32), b64.to(torch.int32)
+    c = torch.empty(plan.total, dtype=torch.int64, device=dev)
+    err = torch.zeros(1, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    plan.capture(a, b, c, err, s)
+    groups = []
+    for np_ in sorted(set(n_powers)):
+        idx = [i for i, n in enumerate(n_powers) if n == np_]
+        groups.append((np_, len(idx), int(min(plan.offsets[i] for i in idx))))
+    tabs = {np_: gf.ffnt_tables(np_, "f32", dev) for np_, _, _ in groups}
+    wss = {}
+    for np_, cnt, _ in groups:
+        w, k = gf.split_plan(np_, 16, False)
+        wss[np_] = (torch.empty(max(1, int(gf.lib().gpufft_negacyclic_mul_split_workspace_bytes(np_, cnt, k))),
+                                dtype=torch.uint8, device=dev), (w, k))
+    c_seq = torch.empty_like(c)
+
+    def seq_step():
+        for np_, cnt, o0 in groups:
+            n = 1 << np_
+            ws, limbs = wss[np_]
+            gf.negacyclic_mul_split(a[o0:o0 + cnt * n].view(cnt, n), b[o0:o0 + cnt * n].view(cnt, n),
+                                    out=c_seq[o0:o0 + cnt * n].view(cnt, n), input_bits=16, non_negative=False,
+                                    limbs=limbs, tables=tabs[np_], workspace=ws, stream=s)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            fn()
+        e1.record(s)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ms = timed(lambda: plan.replay(s))
+    ms_seq = timed(seq_step)
+    line = {"value": world * 4096 / (ms * 1e-3), "unit": "products/s", "ms_per_step": ms, "dtype": "f32 split, exact",
+            "timed": "graph replay of the per-class split chains",
+            "max_pre_rounding_error": float(err.item()), "limbs": sorted(set(plan.limbs)),
+            "per_size_sequential": {"value": world * 4096 / (ms_seq * 1e-3), "ms_per_step": ms_seq,
+                                    "identical_outputs": bool(torch.equal(c, c_seq))}}
     plan.close()
     return line
 
@@ -525,6 +579,89 @@ def run_vjp(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls,
     }
 
 
+def run_cc(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, peak, peak_kind):
+    """C_C cyclic products through the reference API: re/im i.i.d. N(0,1), N =
+    2^10, 2^12, 2^14, 2^16, batch sized to ~1 GiB of input, FP32 and FP64; a step is
+    GPU_FFT forward of both operands and GPU_FFT inverse with the product. Each
+    case reports products/s, HBM GB/s of its algorithmic bytes (3 N complex per
+    product) and the relative L2 error of sampled products against an FP64
+    cyclic convolution."""
+    import numpy as np
+    cases = []
+    stream = torch.cuda.current_stream()
+    with clk_cls(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        time.sleep(0.3)
+        t_first = None
+        for tdt, rdt, tag in ((torch.complex128, np.float64, "f64"), (torch.complex64, np.float32, "f32")):
+            for n_power in (10, 12, 14, 16):
+                M = 1 << n_power
+                csz = 16 if tag == "f64" else 8
+                batch = (1 << 30) // (2 * M * csz)
+                g = torch.Generator(device="cpu").manual_seed(SEED + n_power + rank)
+                x = torch.randn(2 * batch * M, dtype=tdt, generator=g)
+                buf = x.to(dev)
+                roots, inv_roots, _ = gf.host_fft_tables(M // 2, tag)
+                d_roots = torch.from_numpy(np.ascontiguousarray(roots)).to(dev)
+                d_inv = torch.from_numpy(np.ascontiguousarray(inv_roots)).to(dev)
+                L = gf.lib()
+                fn = L.gpufft_fft_c2c_f64 if tag == "f64" else L.gpufft_fft_c2c_f32
+
+                def step():
+                    # the ABI call GPU_FFT makes (the Python mirror enforces the
+                    # reference's n_power >= 12; 2^10 goes straight to the ABI)
+                    gf.check(fn(buf.data_ptr(), d_roots.data_ptr(), n_power, 0, 1, 0, 1.0, 0.0, 2 * batch, 0,
+                                None), "GPU_FFT forward")
+                    gf.check(fn(buf.data_ptr(), d_inv.data_ptr(), n_power, 1, 1, 0, 1.0 / M, 0.0, batch, 1,
+                                None), "GPU_FFT inverse")
+                step()
+                torch.cuda.synchronize()
+                errs = []
+                for k in (0, batch - 1):
+                    a = x[k * M:(k + 1) * M].numpy().astype(np.complex128)
+                    b = x[(batch + k) * M:(batch + k + 1) * M].numpy().astype(np.complex128)
+                    want = np.fft.ifft(np.fft.fft(a) * np.fft.fft(b))
+                    got = buf[k * M:(k + 1) * M].cpu().numpy().astype(np.complex128)
+                    errs.append(float(np.linalg.norm(got - want) / np.linalg.norm(want)))
+                buf.copy_(x.to(dev))
+                for _ in range(args.warmup):
+                    step()
+                barrier()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                t0 = time.time()
+                t_first = t_first or t0
+                e0.record(stream)
+                for _ in range(args.steps):
+                    step()
+                e1.record(stream)
+                barrier()
+                t1 = time.time()
+                ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+                rows, ms_traced = traced_kernels(gf, lambda p, q, r: step(), None, None, None, args, stream, torch,
+                                                 barrier, max_over_ranks)
+                alg = 3 * M * csz * batch
+                cases.append({"dtype": tag, "ring_log2": n_power, "batch": batch, "ms_per_step": ms,
+                              "products_s": world * batch / (ms * 1e-3), "achieved_gbs": alg / (ms * 1e-3) / 1e9,
+                              "frac": alg / (ms * 1e-3) / 1e9 / peak, "rel_l2_vs_fp64_cpu": max(errs),
+                              "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps)})
+                del x, buf
+                torch.cuda.empty_cache()
+        t_last = time.time()
+    head = [c for c in cases if c["dtype"] == "f64" and c["ring_log2"] == 16][0]
+    return {
+        "metric": "C_C cyclic products/s at N=2^16 (FP64), with HBM GB/s per size",
+        "value": head["products_s"], "unit": "products/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded i.i.d. N(0,1) re and im)",
+        "config": {"workload": "C_C cyclic products through GPU_FFT (forward of 2B, inverse with product), "
+                               "N = 2^10..2^16, batch ~1 GiB of input per size, FP32 and FP64",
+                   "l2": "inputs larger than L2 (no flush)"},
+        "roofline": head["roofline"], "cases": cases,
+        "gpu_launches": int(round(sum(k["launches_per_step"] for c in cases for k in c["roofline"]["kernels"])
+                                  * args.steps)),
+        "clocks": clk.summary(t_first, t_last),
+    }
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -559,8 +696,8 @@ def main():
         return reduce_max(ms, dist, dev)
 
     peak, peak_kind = peaks()
-    if args.path in ("batch", "vjp"):
-        fn = run_batch if args.path == "batch" else run_vjp
+    if args.path in ("batch", "vjp", "cc"):
+        fn = {"batch": run_batch, "vjp": run_vjp, "cc": run_cc}[args.path]
         line = fn(args, gf, dev, torch, world, rank, barrier, max_over_ranks, ClockSampler, peak, peak_kind)
         if dist is not None:
             dist.barrier()

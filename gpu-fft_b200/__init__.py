@@ -108,6 +108,13 @@ def lib() -> ctypes.CDLL:
         L.gpufft_negacyclic_mul_split_workspace_bytes.argtypes = [i, i, i]
         L.gpufft_negacyclic_mul_split_workspace_bytes.restype = sz
         L.gpufft_negacyclic_mul_split_f32.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, vp, sz, vp, vp]
+        L.gpufft_split_batch_plan_create.argtypes = [vpp, ctypes.POINTER(ctypes.c_int), i, i, i, vp]
+        L.gpufft_split_batch_plan_layout.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll),
+                                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.gpufft_split_batch_plan_execute.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.gpufft_split_batch_plan_capture.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.gpufft_split_batch_plan_replay.argtypes = [vp, vp]
+        L.gpufft_split_batch_plan_destroy.argtypes = [vp]
         L.gpufft_trace_enable.argtypes = [i]
         L.gpufft_trace_collect.argtypes = [i, ctypes.c_char_p, i, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ll), ctypes.POINTER(i)]
@@ -549,3 +556,71 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+class SplitBatchPlan:
+    """Exact (FP32 split) negacyclic products of mixed ring sizes.
+
+    plan = SplitBatchPlan(n_powers, input_bits=16)
+    a_packed = plan.pack([a_0, a_1, ...])            # int32 rows, grouped by size
+    c_packed, err = plan.execute(a_packed, b_packed)   # int64; or capture() once, replay() after
+    c_list = plan.unpack(c_packed)
+    """
+
+    def __init__(self, n_powers, input_bits, non_negative=False, stream=None):
+        import numpy as np
+        self.n_powers = [int(x) for x in n_powers]
+        n = len(self.n_powers)
+        arr = (ctypes.c_int * n)(*self.n_powers)
+        h = ctypes.c_void_p()
+        check(lib().gpufft_split_batch_plan_create(ctypes.byref(h), arr, n, int(input_bits), int(bool(non_negative)),
+                                                   _stream_handle(stream)), "split_batch_plan_create")
+        self.h = h
+        offs = (ctypes.c_longlong * n)()
+        total = ctypes.c_longlong()
+        wb, kb = (ctypes.c_int * n)(), (ctypes.c_int * n)()
+        check(lib().gpufft_split_batch_plan_layout(self.h, offs, ctypes.byref(total), wb, kb),
+              "split_batch_plan_layout")
+        self.offsets = np.array(offs[:], dtype=np.int64)
+        self.total = int(total.value)
+        self.limbs = list(zip(wb[:], kb[:]))
+
+    def pack(self, polys):
+        import torch
+        out = torch.empty(self.total, dtype=torch.int32, device=polys[0].device)
+        for i, p in enumerate(polys):
+            o = int(self.offsets[i])
+            out[o: o + p.numel()].copy_(p.reshape(-1))
+        return out
+
+    def unpack(self, packed):
+        return [packed[int(o): int(o) + (1 << n)] for o, n in zip(self.offsets, self.n_powers)]
+
+    def execute(self, a, b, out=None, err=None, stream=None):
+        import torch
+        if out is None:
+            out = torch.empty(self.total, dtype=torch.int64, device=a.device)
+        if err is None:
+            err = torch.zeros(1, dtype=torch.float32, device=a.device)
+        check(lib().gpufft_split_batch_plan_execute(self.h, _ptr(a), _ptr(b), _ptr(out), _ptr(err),
+                                                    _stream_handle(stream)), "split_batch_plan_execute")
+        return out, err
+
+    def capture(self, a, b, out, err, stream):
+        check(lib().gpufft_split_batch_plan_capture(self.h, _ptr(a), _ptr(b), _ptr(out), _ptr(err),
+                                                    _stream_handle(stream)), "split_batch_plan_capture")
+
+    def replay(self, stream):
+        check(lib().gpufft_split_batch_plan_replay(self.h, _stream_handle(stream)), "split_batch_plan_replay")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpufft_split_batch_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

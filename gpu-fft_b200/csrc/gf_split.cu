@@ -3,6 +3,9 @@
 #include "gf_split.cuh"
 #include "gf_pipe.cuh"
 
+#include <map>
+#include <vector>
+
 namespace gfb
 {
 
@@ -342,4 +345,206 @@ extern "C" int gpufft_negacyclic_mul_split_f32_host(const int32_t* a, const int3
     return gfb::split_mul_host(a, b, c, n_power, batch, chunk, input_bits, non_negative, limb_bits, num_limbs, tables,
                                workspace, workspace_bytes, reinterpret_cast<unsigned*>(max_error),
                                (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed ring sizes, exact: the split product over a packed batch of requests
+// of different ring sizes. Requests are grouped by size (class-major, original
+// order inside a class, the same layout as gpufft_batch_plan); each class runs
+// the split chain with its own limb plan and twiddles, all on one stream, and
+// capture/replay puts the whole batch in one CUDA graph.
+// ---------------------------------------------------------------------------
+namespace gfb
+{
+struct SplitClass
+{
+    int n_power, w, k;
+    long long count, off; // requests, coefficient offset of the class
+    size_t tab_off;       // complex-float offset of its twiddle block
+};
+
+struct SplitBatchPlan
+{
+    int input_bits = 0, non_negative = 0, count = 0, device = 0;
+    std::vector<int> n_powers;
+    std::vector<long long> offsets;
+    std::vector<SplitClass> classes;
+    long long total = 0;
+    void* d_tabs = nullptr;
+    void* d_ws = nullptr;
+    size_t ws_bytes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+static void free_split_plan(SplitBatchPlan* P)
+{
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    cudaFree(P->d_tabs);
+    cudaFree(P->d_ws);
+    delete P;
+}
+
+static int split_batch_create(SplitBatchPlan** out, const int* n_powers, int count, int input_bits, int non_negative,
+                              cudaStream_t s)
+{
+    if (!out || !n_powers || count <= 0 || input_bits < 1 || input_bits > 31) return GPUFFT_ERROR_INVALID_VALUE;
+    for (int i = 0; i < count; i++)
+        if (n_powers[i] < 2 || n_powers[i] > 22) return GPUFFT_ERROR_INVALID_N_POWER;
+    auto* P = new SplitBatchPlan();
+    P->input_bits = input_bits;
+    P->non_negative = non_negative != 0;
+    P->count = count;
+    P->n_powers.assign(n_powers, n_powers + count);
+    P->offsets.assign(count, 0);
+    cudaGetDevice(&P->device);
+    std::map<int, std::vector<int>> by;
+    for (int i = 0; i < count; i++) by[n_powers[i]].push_back(i);
+    long long coef = 0;
+    size_t tab = 0, ws = 0;
+    for (auto& kv : by)
+    {
+        SplitClass C{};
+        C.n_power = kv.first;
+        if (!choose_limbs(C.n_power, input_bits, P->non_negative, &C.w, &C.k))
+        {
+            delete P;
+            return GPUFFT_ERROR_INVALID_VALUE;
+        }
+        C.count = (long long)kv.second.size();
+        C.off = coef;
+        C.tab_off = tab;
+        for (int r : kv.second)
+        {
+            P->offsets[r] = coef;
+            coef += 1LL << C.n_power;
+        }
+        tab += gpufft_ffnt_tables_count(C.n_power);
+        const int m = C.n_power - 1;
+        ws = std::max(ws, split_ws_bytes(m, C.k, split_wave(m, C.k, C.count)));
+        P->classes.push_back(C);
+    }
+    P->total = coef;
+    P->ws_bytes = ws;
+    cudaError_t e = cudaMalloc(&P->d_tabs, tab * sizeof(cx<float>));
+    if (e == cudaSuccess) e = cudaMalloc(&P->d_ws, std::max<size_t>(ws, 256));
+    if (e != cudaSuccess)
+    {
+        free_split_plan(P);
+        return set_cuda_error(e);
+    }
+    for (const SplitClass& C : P->classes)
+    {
+        const int st = gpufft_ffnt_make_tables_f32(C.n_power, static_cast<cx<float>*>(P->d_tabs) + C.tab_off, s);
+        if (st)
+        {
+            free_split_plan(P);
+            return st;
+        }
+    }
+    *out = P;
+    return GPUFFT_SUCCESS;
+}
+
+static int split_batch_execute(SplitBatchPlan* P, const int32_t* a, const int32_t* b, int64_t* c, unsigned* max_err,
+                               cudaStream_t s)
+{
+    if (!a || !b || !c) return GPUFFT_ERROR_INVALID_VALUE;
+    bool first = true;
+    for (const SplitClass& C : P->classes)
+    {
+        const int st = split_mul(a + C.off, b + C.off, c + C.off, C.n_power, (int)C.count, P->input_bits,
+                                 P->non_negative, C.w, C.k, static_cast<cx<float>*>(P->d_tabs) + C.tab_off, P->d_ws,
+                                 P->ws_bytes, max_err, s, first);
+        if (st) return st;
+        first = false;
+    }
+    return GPUFFT_SUCCESS;
+}
+} // namespace gfb
+
+struct gpufft_split_batch_plan_s
+{
+    gfb::SplitBatchPlan* p;
+};
+
+extern "C" int gpufft_split_batch_plan_create(gpufft_split_batch_plan* plan, const int* n_powers, int count,
+                                              int input_bits, int non_negative, gpufft_stream_t stream)
+{
+    if (!plan) return GPUFFT_ERROR_INVALID_VALUE;
+    gfb::SplitBatchPlan* P = nullptr;
+    const int st = gfb::split_batch_create(&P, n_powers, count, input_bits, non_negative, (cudaStream_t)stream);
+    if (st) return st;
+    *plan = new gpufft_split_batch_plan_s{P};
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_split_batch_plan_layout(gpufft_split_batch_plan plan, long long* offsets, long long* total,
+                                              int* limb_bits, int* num_limbs)
+{
+    if (!plan || !offsets || !total) return GPUFFT_ERROR_INVALID_VALUE;
+    const gfb::SplitBatchPlan* P = plan->p;
+    for (int i = 0; i < P->count; i++)
+    {
+        offsets[i] = P->offsets[i];
+        if (limb_bits || num_limbs)
+            for (const auto& C : P->classes)
+                if (C.n_power == P->n_powers[i])
+                {
+                    if (limb_bits) limb_bits[i] = C.w;
+                    if (num_limbs) num_limbs[i] = C.k;
+                }
+    }
+    *total = P->total;
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_split_batch_plan_execute(gpufft_split_batch_plan plan, const int32_t* a, const int32_t* b,
+                                               int64_t* c, float* max_error, gpufft_stream_t stream)
+{
+    if (!plan) return GPUFFT_ERROR_INVALID_VALUE;
+    return gfb::split_batch_execute(plan->p, a, b, c, reinterpret_cast<unsigned*>(max_error), (cudaStream_t)stream);
+}
+
+extern "C" int gpufft_split_batch_plan_capture(gpufft_split_batch_plan plan, const int32_t* a, const int32_t* b,
+                                               int64_t* c, float* max_error, gpufft_stream_t stream)
+{
+    if (!plan || !stream) return GPUFFT_ERROR_INVALID_VALUE;
+    gfb::SplitBatchPlan* P = plan->p;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    P->exec = nullptr;
+    P->graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return gfb::set_cuda_error(e);
+    const int st = gfb::split_batch_execute(P, a, b, c, reinterpret_cast<unsigned*>(max_error), s);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(s, &g);
+    if (st)
+    {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return gfb::set_cuda_error(e);
+    P->graph = g;
+    e = cudaGraphInstantiate(&P->exec, g, 0);
+    if (e != cudaSuccess) return gfb::set_cuda_error(e);
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_split_batch_plan_replay(gpufft_split_batch_plan plan, gpufft_stream_t stream)
+{
+    if (!plan || !plan->p->exec) return GPUFFT_ERROR_INVALID_VALUE;
+    const cudaError_t e = cudaGraphLaunch(plan->p->exec, (cudaStream_t)stream);
+    return e == cudaSuccess ? GPUFFT_SUCCESS : gfb::set_cuda_error(e);
+}
+
+extern "C" int gpufft_split_batch_plan_destroy(gpufft_split_batch_plan plan)
+{
+    if (!plan) return GPUFFT_ERROR_INVALID_VALUE;
+    gfb::free_split_plan(plan->p);
+    delete plan;
+    return GPUFFT_SUCCESS;
 }

@@ -265,6 +265,27 @@ int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* b, int64_t*
                                     int input_bits, int non_negative, int limb_bits, int num_limbs,
                                     const void* tables, void* workspace, size_t workspace_bytes,
                                     float* max_error, gpufft_stream_t stream);
+/* Mixed ring sizes, exact (no reference counterpart): the split product over
+ * a packed batch of requests of different ring sizes (N = 4 .. 2^22). Requests
+ * are grouped by size, class-major with the original order inside a class;
+ * _layout gives each request's coefficient offset in the packed int32 inputs
+ * and int64 output, the packed length, and each request's limb plan. Each
+ * class runs the split chain with its own limbs and twiddles on one stream;
+ * _capture records one execution on these buffers as a CUDA graph (non-default
+ * stream) that _replay launches. max_error (device, may be NULL) covers every
+ * class. The plan owns its twiddles and workspace. */
+typedef struct gpufft_split_batch_plan_s* gpufft_split_batch_plan;
+int gpufft_split_batch_plan_create(gpufft_split_batch_plan* plan, const int* n_powers, int count, int input_bits,
+                                   int non_negative, gpufft_stream_t stream);
+int gpufft_split_batch_plan_layout(gpufft_split_batch_plan plan, long long* offsets, long long* total,
+                                   int* limb_bits, int* num_limbs);
+int gpufft_split_batch_plan_execute(gpufft_split_batch_plan plan, const int32_t* a, const int32_t* b, int64_t* c,
+                                    float* max_error, gpufft_stream_t stream);
+int gpufft_split_batch_plan_capture(gpufft_split_batch_plan plan, const int32_t* a, const int32_t* b, int64_t* c,
+                                    float* max_error, gpufft_stream_t stream);
+int gpufft_split_batch_plan_replay(gpufft_split_batch_plan plan, gpufft_stream_t stream);
+int gpufft_split_batch_plan_destroy(gpufft_split_batch_plan plan);
+
 /* The same product on host buffers, chunked with overlapped transfers exactly
  * like gpufft_negacyclic_mul_f64_host; max_error (device) covers all chunks. */
 size_t gpufft_negacyclic_mul_split_f32_host_workspace_bytes(int n_power, int batch, int chunk, int num_limbs);

@@ -84,3 +84,42 @@ def test_batch_4096_mixed_sizes_graph_and_autotune(gf, dev):
     assert torch.equal(c0, c1)
     assert plan.status() == 0
     plan.close()
+
+
+def test_split_batch_exact_and_graph(gf, O, dev):
+    # exact mixed-size products (FP32 split): every request equals the per-size
+    # split call bit for bit and the exact negacyclic product on sampled
+    # coefficients; a captured graph replays to the same output
+    rng = np.random.default_rng(45)
+    n_powers = make_requests(rng, 60, 2, 17)
+    plan = gf.SplitBatchPlan(n_powers, input_bits=16, non_negative=False)
+    a_list = [torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, 1 << n).astype(np.int32)).to(dev)
+              for n in n_powers]
+    b_list = [torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, 1 << n).astype(np.int32)).to(dev)
+              for n in n_powers]
+    a, b = plan.pack(a_list), plan.pack(b_list)
+    c, err = plan.execute(a, b)
+    assert float(err.item()) < 0.5
+    got = plan.unpack(c)
+    for np_ in sorted(set(n_powers)):
+        idx = [i for i, n in enumerate(n_powers) if n == np_]
+        C = gf.negacyclic_mul_split(torch.stack([a_list[i] for i in idx]), torch.stack([b_list[i] for i in idx]),
+                                    input_bits=16, non_negative=False)
+        for k, i in enumerate(idx):
+            assert torch.equal(got[i], C[k]), (i, np_)
+    for i in rng.choice(len(n_powers), 8, replace=False):
+        n = 1 << n_powers[i]
+        ai, bi = a_list[i].cpu().numpy(), b_list[i].cpu().numpy()
+        idx = np.sort(rng.choice(n, min(n, 64), replace=False)).astype(np.int32)
+        assert np.array_equal(got[i].cpu().numpy()[idx], O.wrap64(O.negacyclic_coeffs(ai, bi, idx)))
+    s = torch.cuda.Stream()
+    c2 = torch.empty_like(c)
+    err2 = torch.zeros(1, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    plan.capture(a, b, c2, err2, s)
+    plan.replay(s)
+    plan.replay(s)
+    s.synchronize()
+    assert torch.equal(c2, c)
+    assert float(err2.item()) == float(err.item())
+    plan.close()

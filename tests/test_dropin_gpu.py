@@ -42,7 +42,7 @@ def fft_table(O, n_power, T, neg=False, inverse=False):
     return (ri if inverse else r), ninv
 
 
-C2C_SIZES = [1, 2, 3, 5, 8, 11, 12, 13, 15, 16, 17, 20, 22]
+C2C_SIZES = [1, 2, 3, 5, 8, 10, 11, 12, 13, 14, 15, 16, 17, 20, 22]
 
 
 @pytest.mark.parametrize("T", [np.float64, np.float32])
@@ -223,3 +223,33 @@ def test_reference_range_ends(gf, O, dev, n_power):
     with pytest.raises(ValueError, match="Invalid n_power range!"):
         gf.GPU_FFT(buf, td(roots, dev), gf.fft_configuration(n_power=n_power + (1 if n_power == 24 else -1)), 1,
                    False)
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+@pytest.mark.parametrize("n_power", [10, 12, 14, 16])
+def test_c2c_cyclic_product_gib_batch(gf, O, dev, T, n_power):
+    # the C_C product workload: re/im i.i.d. N(0,1), batch sized to ~1 GiB of
+    # input; forward of 2 batch, inverse with the product; sampled products
+    # against an FP64 cyclic convolution (numpy FFT)
+    M = 1 << n_power
+    C = cdt(T)
+    csz = np.dtype(C).itemsize
+    batch = (1 << 30) // (2 * M * csz)
+    g = torch.Generator(device="cpu").manual_seed(2000 + n_power)
+    tdt = torch.complex128 if T == np.float64 else torch.complex64
+    x = torch.randn(2 * batch * M, dtype=tdt, generator=g)
+    buf = x.to(dev)
+    roots, _ = fft_table(O, n_power, T)
+    inv_roots, _ = fft_table(O, n_power, T, inverse=True)
+    d_roots, d_inv = td(roots, dev), td(inv_roots, dev)
+    L = gf.lib()
+    f = L.gpufft_fft_c2c_f64 if T == np.float64 else L.gpufft_fft_c2c_f32
+    gf.check(f(buf.data_ptr(), d_roots.data_ptr(), n_power, 0, 1, 0, 1.0, 0.0, 2 * batch, 0, None), "fwd")
+    gf.check(f(buf.data_ptr(), d_inv.data_ptr(), n_power, 1, 1, 0, 1.0 / M, 0.0, batch, 1, None), "inv")
+    for k in (0, batch // 2, batch - 1):
+        a = x[k * M:(k + 1) * M].numpy().astype(np.complex128)
+        b = x[(batch + k) * M:(batch + k + 1) * M].numpy().astype(np.complex128)
+        want = np.fft.ifft(np.fft.fft(a) * np.fft.fft(b))
+        got = buf[k * M:(k + 1) * M].cpu().numpy()
+        assert rel_l2(got, want) < (1e-13 if T == np.float64 else 2e-6) * n_power
+
