@@ -99,6 +99,7 @@ def lib() -> ctypes.CDLL:
         L.gpufft_batch_plan_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_char_p, vp]
         L.gpufft_batch_plan_capture.argtypes = [vp, vp, vp, vp, vp]
         L.gpufft_batch_plan_replay.argtypes = [vp, vp]
+        L.gpufft_batch_plan_set_shape.argtypes = [vp, i, i]
         L.gpufft_batch_plan_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ll)]
         L.gpufft_batch_plan_status.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
@@ -535,11 +536,16 @@ class BatchPlan:
     def replay(self, stream):
         check(lib().gpufft_batch_plan_replay(self.h, _stream_handle(stream)), "batch_plan_replay")
 
+    def set_shape(self, ctas_per_sm, items_per_grab=1):
+        """Persistent launch (ctas_per_sm 1 or 2) or per-class chains (0)."""
+        check(lib().gpufft_batch_plan_set_shape(self.h, int(ctas_per_sm), int(items_per_grab)), "batch_plan_set_shape")
+
     def info(self):
         m, g, gr, ws = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
         check(lib().gpufft_batch_plan_info(self.h, ctypes.byref(m), ctypes.byref(g), ctypes.byref(gr),
                                            ctypes.byref(ws)), "batch_plan_info")
-        return {"ctas_per_sm": m.value, "items_per_grab": g.value, "grid": gr.value, "workspace_bytes": ws.value}
+        return {"mode": "persistent" if m.value else "per-class chains", "ctas_per_sm": m.value,
+                "items_per_grab": g.value, "grid": gr.value, "workspace_bytes": ws.value}
 
     def status(self):
         f = ctypes.c_int()

@@ -25,8 +25,10 @@
 // reports the flag.
 //
 // Autotuning: the launch shape (CTAs per SM, and how many work items a CTA
-// takes per counter update) is timed on the caller's data and the fastest is
-// kept, cached in a JSON file keyed by GPU name, driver version and precision.
+// takes per counter update) and, as one more candidate, per-class fused chains
+// instead of the persistent kernel, are timed on the caller's data and the
+// fastest is kept, cached in a JSON file keyed by GPU name, driver version,
+// precision and the size histogram.
 #include "gf_fused.cuh"
 
 #include <cmath>
@@ -301,8 +303,43 @@ template <typename T, int MINB> static int batch_launch(BatchPlan* P, const void
     return check_launch();
 }
 
+// The other execution mode: one fused product chain per size class (the
+// single-size entry point on the class's rows, twiddles and workspace),
+// launched back to back on the stream. The persistent kernel keeps one CTA of
+// 8 warps per SM for every phase (its fused middle needs the registers), while
+// the per-class chains run their first and last passes as high-occupancy
+// column kernels; the autotuner times both.
+static int class_chains(BatchPlan* P, const void* a, const void* b, void* c, cudaStream_t s)
+{
+    const size_t cxb = P->precision == 64 ? 16 : 8, eb = cxb / 2;
+    for (const BatchClass& C : P->classes)
+    {
+        const long long M = 1LL << C.m;
+        const char* pa = static_cast<const char*>(a) + C.coef_off * eb;
+        const char* pb = static_cast<const char*>(b) + C.coef_off * eb;
+        char* pc = static_cast<char*>(c) + C.coef_off * eb;
+        const void* tab = static_cast<const char*>(P->d_tabs) + C.tab_off * cxb;
+        void* ws = C.m > EBITS ? static_cast<char*>(P->d_ws) + C.ws_off * cxb : nullptr;
+        const size_t wsb = C.m > EBITS ? (size_t)(2 * C.count * M) * cxb : 0;
+        const int st = P->precision == 64
+                           ? gpufft_negacyclic_mul_f64(reinterpret_cast<const double*>(pa),
+                                                       reinterpret_cast<const double*>(pb),
+                                                       reinterpret_cast<double*>(pc), C.m + 1, (int)C.count, tab, ws,
+                                                       wsb, s)
+                           : gpufft_negacyclic_mul_f32(reinterpret_cast<const float*>(pa),
+                                                       reinterpret_cast<const float*>(pb),
+                                                       reinterpret_cast<float*>(pc), C.m + 1, (int)C.count, tab, ws,
+                                                       wsb, s);
+        if (st) return st;
+    }
+    return GPUFFT_SUCCESS;
+}
+
+// minb 0 selects the per-class chains; 1 or 2 the persistent kernel with that
+// many CTAs per SM.
 static int batch_execute(BatchPlan* P, const void* a, const void* b, void* c, cudaStream_t s)
 {
+    if (P->minb == 0) return class_chains(P, a, b, c, s);
     if (P->precision == 64) return P->minb == 2 ? batch_launch<double, 2>(P, a, b, c, s) : batch_launch<double, 1>(P, a, b, c, s);
     return P->minb == 2 ? batch_launch<float, 2>(P, a, b, c, s) : batch_launch<float, 1>(P, a, b, c, s);
 }
@@ -464,7 +501,7 @@ static bool cache_lookup(const char* path, const std::string& key, int* minb, in
         if (a == std::string::npos || b == std::string::npos) continue;
         mb = std::atoi(line.c_str() + a + 8);
         gb = std::atoi(line.c_str() + b + 8);
-        if ((mb == 1 || mb == 2) && gb >= 1 && gb <= 8)
+        if ((mb == 0 || mb == 1 || mb == 2) && gb >= 1 && gb <= 8)
         {
             *minb = mb;
             *grab = gb;
@@ -496,11 +533,12 @@ static int autotune(BatchPlan* P, const void* a, const void* b, void* c, const c
         return set_cuda_error(cudaGetLastError());
     float best = 1e30f;
     int bmb = 1, bgb = 1;
-    const int minbs[2] = {1, 2};
+    const int minbs[3] = {1, 2, 0};
     const int grabs[3] = {1, 2, 4};
     for (int mbv : minbs)
         for (int gbv : grabs)
         {
+            if (mbv == 0 && gbv != 1) continue; // per-class chains take no grab size
             P->minb = mbv;
             P->grab = gbv;
             int st = batch_execute(P, a, b, c, s); // warm-up (also checks the shape launches)
@@ -606,6 +644,16 @@ extern "C" int gpufft_batch_plan_replay(gpufft_batch_plan plan, gpufft_stream_t 
     if (!P->exec) return GPUFFT_ERROR_INVALID_VALUE;
     const cudaError_t e = cudaGraphLaunch(P->exec, (cudaStream_t)stream);
     return e == cudaSuccess ? GPUFFT_SUCCESS : gfb::set_cuda_error(e);
+}
+
+extern "C" int gpufft_batch_plan_set_shape(gpufft_batch_plan plan, int ctas_per_sm, int items_per_grab)
+{
+    if (!plan || ctas_per_sm < 0 || ctas_per_sm > 2 || items_per_grab < 1 || items_per_grab > 8)
+        return GPUFFT_ERROR_INVALID_VALUE;
+    auto* P = reinterpret_cast<gfb::BatchPlan*>(plan);
+    P->minb = ctas_per_sm;
+    P->grab = ctas_per_sm == 0 ? 1 : items_per_grab;
+    return GPUFFT_SUCCESS;
 }
 
 extern "C" int gpufft_batch_plan_info(gpufft_batch_plan plan, int* ctas_per_sm, int* items_per_grab, int* grid,

@@ -17,11 +17,8 @@ enum InKind
     IN_FOLD2 = 4, // IN_FOLD with batch entries [0, split) from `in`, the rest from `in2`
     IN_LIN2 = 5,  // zero-padded linear operand: x_j = f_j (real, rows of M), then twist;
                   // batch entries [0, split) from `in`, the rest from `in2`
-    IN_VJP3 = 6,  // batch entries [0, split): IN_FOLD from `in` (rows of 2M);
+    IN_VJP3 = 6   // batch entries [0, split): IN_FOLD from `in` (rows of 2M);
                   // [split, 2 split): IN_LIN from `in2`; [2 split, 3 split): IN_LIN from `in3`
-    IN_GROUP = 7  // split product: transform b = s W + p is the limb group
-                  // C^_s = sum_{i+j=s} A^_i B^_j (+ centring term) of product p,
-                  // from the limb spectra [2k][W][M] at `in`
 };
 enum OutKind
 {
@@ -59,11 +56,6 @@ template <typename T> struct PassArgs
     int in_kind, out_kind;
     int zero_pad; // forward first pass: the upper half of each input is zero
     int do_scale; // last inverse pass: multiply by scale
-    // IN_GROUP (split product)
-    long long W;          // products per wave
-    const cx<T>* uspec;   // transform of the all-ones polynomial
-    int gk, gcentre;      // limbs; centred inputs
-    int uq, ur;           // centring term joins group l + uq, scaled by 2^ur
 };
 
 // Where the 16 registers of thread t (window W) live: batch entry b[r] and
@@ -162,30 +154,6 @@ __device__ __forceinline__ cx<T> load_elem(const PassArgs<T>& a, int kind, long 
         const T* base = reinterpret_cast<const T*>(b < 2 * a.split ? a.in2 : a.in3);
         b -= (b < 2 * a.split) ? a.split : 2 * a.split;
         return cmul<T>(mk<T>(ld_stream(base + b * M + j), T(0)), ldg<T>(a.twist + j));
-    }
-    else if (kind == IN_GROUP)
-    {
-        const long long sg = b / a.W, p = b - sg * a.W;
-        const cx<T>* sp = reinterpret_cast<const cx<T>*>(a.in) + p * M + j;
-        const long long st = a.W * M; // stride between limb spectra
-        const int k = a.gk;
-        const int i0 = (int)sg - (k - 1) > 0 ? (int)sg - (k - 1) : 0;
-        cx<T> acc = mk<T>(T(0), T(0));
-        constexpr int KMAX = 8;
-#pragma unroll
-        for (int ii = 0; ii < KMAX; ii++)
-        {
-            const int i = i0 + ii;
-            if (i <= (int)sg && i < k) acc = cadd<T>(acc, cmul<T>(sp[i * st], sp[(k + sg - i) * st]));
-        }
-        const int l = (int)sg - a.uq;
-        if (a.gcentre && l >= 0 && l < k)
-        {
-            const cx<T> e = cadd<T>(sp[l * st], sp[(k + l) * st]);
-            const T sc = (T)(1 << a.ur);
-            acc = cadd<T>(acc, cmul<T>(mk<T>(e.x * sc, e.y * sc), ldg<T>(a.uspec + j)));
-        }
-        return acc;
     }
     else
     {
@@ -392,7 +360,6 @@ template <typename T> inline double pass_alg_bytes(const PassArgs<T>& a)
     case IN_LIN2: in = t; break;
     case IN_VJP3: in = 4 * t / 3; break;
     case IN_PROD: in = 2 * c; break;
-    case IN_GROUP: in = 2 * a.gk * c; break;
     case IN_CPX: in = a.zero_pad ? c / 2 : c; break;
     default: break;
     }
@@ -416,13 +383,14 @@ inline const char* kind_name(int fwd) { return fwd ? "fwd" : "inv"; }
 constexpr int COL_MAX_L = 4;
 constexpr int COL_THREADS = 128;
 
+// Column `idx` (over all batch entries) of the pass; no shared memory, no
+// barrier, so it can run inside a persistent kernel too.
 template <typename T, bool FWD, int L, int IK, int OK>
-__global__ void __launch_bounds__(COL_THREADS) col_pass_kernel(const PassArgs<T> a)
+__device__ __forceinline__ void col_pass_body(const PassArgs<T>& a, long long idx)
 {
     constexpr int R = 1 << L;
     const int m = a.geo.m, s0 = a.geo.s0;
     const int lc = m - s0 - L; // log2 columns per group
-    const long long idx = (long long)blockIdx.x * COL_THREADS + threadIdx.x;
     const long long b = idx >> (m - L);
     if (b >= a.batch) return;
     const long long r = idx & ((1LL << (m - L)) - 1);
@@ -451,6 +419,12 @@ __global__ void __launch_bounds__(COL_THREADS) col_pass_kernel(const PassArgs<T>
     }
 #pragma unroll
     for (int i = 0; i < R; i++) store_elem<T>(a, OK, b, j0 + i * C, x[i]);
+}
+
+template <typename T, bool FWD, int L, int IK, int OK>
+__global__ void __launch_bounds__(COL_THREADS) col_pass_kernel(const PassArgs<T> a)
+{
+    col_pass_body<T, FWD, L, IK, OK>(a, (long long)blockIdx.x * COL_THREADS + threadIdx.x);
 }
 
 // Launch the column form when a kernel for (in_kind, out_kind) is compiled:

@@ -141,6 +141,10 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         long long hoff = 0; // 2^(w-1) (1 + 2^w + ... + 2^(w(k-2)))
         for (int i = 0; i + 1 < k; i++) hoff += 1LL << (w * i + w - 1);
         A.voff = hoff - A.K;
+        unsigned long long S = 0; // sum_{l<k-1} 2^(w l)
+        for (int i = 0; i + 1 < k; i++) S += 1ULL << (w * i);
+        const unsigned long long K = (unsigned long long)A.K;
+        A.uucoef = (long long)(K * K - K * S);
     }
 
     // the workspace sets the wave (as many products as it holds, rounded to

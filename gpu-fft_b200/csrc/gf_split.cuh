@@ -69,6 +69,7 @@ struct SplitArgs
     const cx<float>* uspec; // transform of the all-ones polynomial (table block)
     long long K;       // centring offset subtracted from every coefficient (0: none)
     long long voff;    // split_digit offset minus K: V = x + voff for a raw coefficient x
+    long long uucoef;  // K^2 - K S (mod 2^64): exact int64 u*u correction (uu_term)
     int uq, ur;        // K = 2^(w uq + ur): centring term joins groups s = l + uq, scaled 2^ur
     float scale;
     int w, k;
@@ -105,9 +106,18 @@ __device__ __forceinline__ void report_err(unsigned* dst, float e)
 // i.e. 2^r (E^a_l + E^b_l) U joins limb group s = l + q in the frequency domain
 // (U = transform of u, part of the native table block), and K^2 u u, whose
 // coefficients are K^2 (2k + 2 - N), is added exactly in int64 at the end.
+//
+// Balanced digits below the top one have mean -1/2 on uniformly spread
+// values (the top digit, which takes what is left, has mean ~0), so for
+// l < k-1, e^a_l + e^b_l drifts by -u and (e^a_l + e^b_l) u grows like N/2 --
+// eight times the group values the limb plan is sized for at N = 2^16. For
+// those limbs the frequency domain carries 2^r (E^a_l + E^b_l + U) U instead,
+// the transform of a zero-mean integer polynomial times u, and the extra
+// sum_{l<k-1} 2^(w (l + q) + r) u u = K S u u (S = sum_{l<k-1} 2^(w l)) is
+// subtracted exactly in int64 with the K^2 term: uucoef = K^2 - K S.
 __device__ __forceinline__ long long uu_term(const SplitArgs& a, long long k, long long N)
 {
-    return (long long)((unsigned long long)a.K * (unsigned long long)a.K * (unsigned long long)(2 * k + 2 - N));
+    return (long long)((unsigned long long)a.uucoef * (unsigned long long)(2 * k + 2 - N));
 }
 
 // --------------------------------------------------------------------------
@@ -252,7 +262,8 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
                     for (int ll = 0; ll < K; ll++)
                         if (ll == l)
                         {
-                            const cx<float> e = cadd<float>(v[ll][q], v[K + ll][q]);
+                            cx<float> e = cadd<float>(v[ll][q], v[K + ll][q]);
+                            if (ll < K - 1) e = cadd<float>(e, u[q]);
                             acc = cadd<float>(acc, cmul<float>(mk<float>(e.x * uscale, e.y * uscale), u[q]));
                         }
                 }
@@ -517,7 +528,8 @@ template <int K> __global__ void __launch_bounds__(256) split_groups(const Split
             for (int l = 0; l < K; l++)
                 if (l + a.uq == s)
                 {
-                    const cx<float> e = cadd<float>(v[l], v[K + l]);
+                    cx<float> e = cadd<float>(v[l], v[K + l]);
+                    if (l < K - 1) e = cadd<float>(e, u);
                     acc = cadd<float>(acc, cmul<float>(mk<float>(e.x * uscale, e.y * uscale), u));
                 }
         }

@@ -216,13 +216,19 @@ int gpufft_batch_plan_create(gpufft_batch_plan* plan, const int* n_powers, int c
  * size. order[k] is the request stored k-th, offsets[i] the coefficient offset
  * of request i in the packed arrays, *total their length. Any may be NULL. */
 int gpufft_batch_plan_layout(gpufft_batch_plan plan, int* order, long long* offsets, long long* total);
-/* c = a * b for every request, in one persistent launch on `stream`. */
+/* c = a * b for every request on `stream`: one persistent launch, or (when
+ * the autotuner found it faster) one fused chain per ring-size class. */
 int gpufft_batch_plan_execute(gpufft_batch_plan plan, const void* a, const void* b, void* c, gpufft_stream_t stream);
-/* Time the candidate launch shapes (CTAs per SM, work items per grab) on these
- * buffers and keep the fastest; cache_path (may be NULL) is a JSON-lines file
- * of earlier results keyed by GPU, driver, precision and size histogram. */
+/* Time the candidates on these buffers and keep the fastest: the persistent
+ * launch with 1 or 2 CTAs per SM and 1, 2 or 4 work items per grab, and the
+ * per-class fused chains (reported as 0 CTAs per SM by _info). cache_path (may
+ * be NULL) is a JSON-lines file of earlier results keyed by GPU, driver,
+ * precision and size histogram. */
 int gpufft_batch_plan_autotune(gpufft_batch_plan plan, const void* a, const void* b, void* c,
                                const char* cache_path, gpufft_stream_t stream);
+/* Choose the execution mode by hand: ctas_per_sm 1 or 2 (persistent launch,
+ * items_per_grab 1..8), or 0 (per-class fused chains). */
+int gpufft_batch_plan_set_shape(gpufft_batch_plan plan, int ctas_per_sm, int items_per_grab);
 /* Capture one execution on these buffers into a CUDA graph held by the plan
  * (stream must be a non-default stream), then launch it with _replay. */
 int gpufft_batch_plan_capture(gpufft_batch_plan plan, const void* a, const void* b, void* c, gpufft_stream_t stream);

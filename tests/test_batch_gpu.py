@@ -41,11 +41,13 @@ def test_batch_matches_per_size_launches(gf, O, dev, dtype):
     b_list = [torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, 1 << n).astype(np.float64)).to(dev, dtype)
               for n in n_powers]
     a, b = plan.pack(a_list), plan.pack(b_list)
-    c = plan.execute(a, b)
     ref = per_size_reference(gf, plan, a_list, b_list, dtype)
-    got = plan.unpack(c)
-    for i in range(len(n_powers)):
-        assert torch.equal(got[i], ref[i]), (i, n_powers[i])
+    for shape in ((1, 1), (2, 4), (0, 1)):  # persistent launches and per-class chains
+        plan.set_shape(*shape)
+        c = plan.execute(a, b)
+        got = plan.unpack(c)
+        for i in range(len(n_powers)):
+            assert torch.equal(got[i], ref[i]), (shape, i, n_powers[i])
     assert plan.status() == 0
     if dtype == torch.float64:  # |c| < 2^47: exact
         for i in rng.choice(len(n_powers), 6, replace=False):
@@ -71,7 +73,7 @@ def test_batch_4096_mixed_sizes_graph_and_autotune(gf, dev):
     with tempfile.TemporaryDirectory() as d:
         cache = os.path.join(d, "tune.jsonl")
         info = plan.autotune(a, b, torch.empty_like(a), cache)
-        assert info["ctas_per_sm"] in (1, 2) and info["items_per_grab"] in (1, 2, 4)
+        assert info["ctas_per_sm"] in (0, 1, 2) and info["items_per_grab"] in (1, 2, 4)
         assert os.path.exists(cache)
         plan.autotune(a, b, torch.empty_like(a), cache)  # cache hit
     s = torch.cuda.Stream()

@@ -61,3 +61,17 @@ def test_split_reports_inexact_plan(gf, dev):
     a = torch.from_numpy(rng.integers(0, 1 << 24, (1, n)).astype(np.int32)).to(dev)
     _, err = gf.negacyclic_mul_split(a, a, input_bits=24, non_negative=True, limbs=(12, 2), return_error=True)
     assert float(err.item()) >= 0.5
+
+
+@pytest.mark.parametrize("n_power,batch", [(16, 64), (17, 32)])
+def test_split_error_margin_uniform_24bit(gf, dev, n_power, batch):
+    # balanced digits of uniform data drift by -1/2; the centring term removes
+    # that drift, so the library's 5-limb plan keeps its error well below 0.5
+    # (without it the report was 0.25 at 2^16 and 0.5 at 2^17)
+    rng = np.random.default_rng(900 + n_power)
+    n = 1 << n_power
+    a = torch.from_numpy(rng.integers(0, 1 << 24, (batch, n)).astype(np.int32)).to(dev)
+    b = torch.from_numpy(rng.integers(0, 1 << 24, (batch, n)).astype(np.int32)).to(dev)
+    assert gf.split_plan(n_power, 24, True) == (5, 5)
+    _, err = gf.negacyclic_mul_split(a, b, input_bits=24, non_negative=True, return_error=True)
+    assert float(err.item()) <= 0.25
