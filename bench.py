@@ -39,8 +39,10 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--path", choices=["split", "f64", "f32", "dropin_f64", "batch", "vjp", "cc"], default="split",
-                   help="split/f64/f32/dropin_f64: N = 2^16 negacyclic products, batch 256, 24-bit coefficients; "
+    p.add_argument("--path", choices=["split", "split64", "f64", "f32", "dropin_f64", "batch", "vjp", "cc"],
+                   default="split",
+                   help="split (exact, FP32 transforms) / split64 (exact, FP64 transforms) / f64 / f32 / dropin_f64: "
+                        "N = 2^16 negacyclic products, batch 256, 24-bit coefficients; "
                         "batch: 4096 mixed ring sizes 2^10..2^17 (one persistent launch in a CUDA "
                         "graph); vjp: FP32 linear convolution N = 2^14, batch 512, forward + VJP; cc: C_C cyclic "
                         "products through GPU_FFT, FP32 and FP64, N = 2^10..2^16, ~1 GiB batches")
@@ -217,6 +219,24 @@ def make_path(gf, name, n_power, batch, dev, torch):
             gf.negacyclic_mul_host(x, y, out=out, tables=tables, workspace=hws)
         dt = torch.float64 if f64 else torch.float32
         return step, host_step, 3 * n * esz, dt, dt, (1 if m <= 12 else 3 * waves)
+    if name == "split64":
+        # the exact product with FP64 transforms (two 12-bit limbs at N = 2^16)
+        w, k = gf.split_plan(n_power, 24, True, "f64")
+        tables = gf.ffnt_tables(n_power, "f64", dev)
+        need = int(gf.lib().gpufft_negacyclic_mul_split_f64_workspace_bytes(n_power, batch, k))
+        ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+
+        def step(x, y, out):
+            gf.negacyclic_mul_split(x, y, out=out, input_bits=24, non_negative=True, limbs=(w, k), tables=tables,
+                                    workspace=ws, precision="f64")
+
+        def host_step(x, y, out):
+            # no host-buffer variant of the FP64 split: copy in, product, copy out
+            xd, yd = x.to(dev, non_blocking=True), y.to(dev, non_blocking=True)
+            od = torch.empty(out.shape, dtype=out.dtype, device=dev)
+            step(xd, yd, od)
+            out.copy_(od, non_blocking=True)
+        return step, host_step, 16 * n, torch.int32, torch.int64, 5
     if name == "split":
         w, k = gf.split_plan(n_power, 24, True)
         tables = gf.ffnt_tables(n_power, "f32", dev)
@@ -706,7 +726,7 @@ def main():
             print(json.dumps(line), flush=True)
         return
     results = {}
-    paths = [args.path] + ([p for p in ("f64",) if p != args.path] if args.compare else [])
+    paths = [args.path] + ([p for p in ("split64", "f64") if p != args.path] if args.compare else [])
     with ClockSampler(local) as clk:
         time.sleep(0.5)  # let the sampler start before the timed regions
         for name in paths:
@@ -725,7 +745,7 @@ def main():
                                  traced_launches=sum(r["launches"] for r in rows),
                                  value=world * batch / (ms * 1e-3), achieved=achieved,
                                  h2d=2 * batch * n * a_host.element_size(), d2h=batch * n * c_host.element_size(),
-                                 dtype={torch.float64: "f64", torch.float32: "f32", torch.int32: "f32"}[din],
+                                 dtype="f64" if name in ("f64", "dropin_f64", "split64") else "f32",
                                  c=c[:2].cpu() if rank == 0 else None)
             del a, b, c, a_host, b_host, c_host
         time.sleep(0.3)

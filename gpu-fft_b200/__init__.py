@@ -109,6 +109,10 @@ def lib() -> ctypes.CDLL:
         L.gpufft_negacyclic_mul_split_workspace_bytes.argtypes = [i, i, i]
         L.gpufft_negacyclic_mul_split_workspace_bytes.restype = sz
         L.gpufft_negacyclic_mul_split_f32.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, vp, sz, vp, vp]
+        L.gpufft_negacyclic_mul_split_f64.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, vp, sz, vp, vp]
+        L.gpufft_split_plan_f64.argtypes = [i, i, i, ip, ip]
+        L.gpufft_negacyclic_mul_split_f64_workspace_bytes.argtypes = [i, i, i]
+        L.gpufft_negacyclic_mul_split_f64_workspace_bytes.restype = sz
         L.gpufft_split_batch_plan_create.argtypes = [vpp, ctypes.POINTER(ctypes.c_int), i, i, i, vp]
         L.gpufft_split_batch_plan_layout.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll),
                                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
@@ -294,18 +298,20 @@ def negacyclic_mul(a, b, out=None, tables=None, workspace=None, stream=None):
     return out
 
 
-def split_plan(n_power: int, input_bits: int, non_negative: bool = False):
-    """(limb_bits, num_limbs) the library uses for exact FP32 split products."""
+def split_plan(n_power: int, input_bits: int, non_negative: bool = False, precision: str = "f32"):
+    """(limb_bits, num_limbs) the library uses for exact split products with
+    FP32 ("f32") or FP64 ("f64") transforms."""
     w, k = ctypes.c_int(), ctypes.c_int()
-    check(lib().gpufft_split_plan(n_power, input_bits, int(non_negative), ctypes.byref(w), ctypes.byref(k)),
-          "split_plan")
+    f = lib().gpufft_split_plan_f64 if precision == "f64" else lib().gpufft_split_plan
+    check(f(n_power, input_bits, int(non_negative), ctypes.byref(w), ctypes.byref(k)), "split_plan")
     return w.value, k.value
 
 
 def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, limbs=None, tables=None,
-                         workspace=None, stream=None, return_error=False):
+                         workspace=None, stream=None, return_error=False, precision="f32"):
     """Exact c = a * b mod (X^N + 1) for (batch, N) int32 tensors, computed with FP32
-    transforms on limbs; returns an int64 tensor (and the max pre-rounding error)."""
+    (precision="f32", N <= 2^22) or FP64 (precision="f64", N <= 2^17) transforms on
+    limbs; returns an int64 tensor (and the max pre-rounding error)."""
     import torch
     batch, n = a.shape
     n_power = n.bit_length() - 1
@@ -316,16 +322,20 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
         mn = int(torch.minimum(a.min(), b.min()).item())
         input_bits = max(1, mx.bit_length()) if input_bits is None else input_bits
         non_negative = (mn >= 0) if non_negative is None else non_negative
-    w, k = limbs if limbs is not None else split_plan(n_power, input_bits, non_negative)
+    f64 = precision == "f64"
+    w, k = limbs if limbs is not None else split_plan(n_power, input_bits, non_negative, precision)
     if tables is None:
-        tables = ffnt_tables(n_power, "f32", a.device, stream)
+        tables = ffnt_tables(n_power, "f64" if f64 else "f32", a.device, stream)
     if out is None:
         out = torch.empty((batch, n), dtype=torch.int64, device=a.device)
-    need = int(lib().gpufft_negacyclic_mul_split_workspace_bytes(n_power, batch, k))
+    L = lib()
+    wsf = L.gpufft_negacyclic_mul_split_f64_workspace_bytes if f64 else L.gpufft_negacyclic_mul_split_workspace_bytes
+    need = int(wsf(n_power, batch, k))
     if workspace is None:
         workspace = torch.empty(max(need, 1), dtype=torch.uint8, device=a.device)
     err = torch.zeros(1, dtype=torch.float32, device=a.device)
-    st = lib().gpufft_negacyclic_mul_split_f32(
+    fn = L.gpufft_negacyclic_mul_split_f64 if f64 else L.gpufft_negacyclic_mul_split_f32
+    st = fn(
         _ptr(a), _ptr(b), _ptr(out), n_power, batch, int(input_bits), int(bool(non_negative)), w, k,
         _ptr(tables), workspace.data_ptr(), workspace.numel() * workspace.element_size(), err.data_ptr(),
         _stream_handle(stream))

@@ -1,5 +1,6 @@
-// gpufft-b200: FP32 split-precision negacyclic product -- host side (plans,
-// workspace, launches) and the C ABI. The kernels are in gf_split.cuh.
+// gpufft-b200: split-precision negacyclic products (FP32 and FP64 transforms,
+// exact int64 results) -- host side (plans, workspace, launches) and the C
+// ABI. The kernels are in gf_split.cuh.
 #include "gf_split.cuh"
 #include "gf_pipe.cuh"
 
@@ -14,15 +15,16 @@ namespace gfb
 // --------------------------------------------------------------------------
 // Largest pre-rounding error expected for k balanced limbs of width w.
 // For one limb pair the measured maximum over a batch follows
-//     err ~ C * rms(d_a) * rms(d_b) * sqrt(N) * sqrt(log2(N/2)) * 2^-24,  C = 7.1
-// (calibrated on FP32 negacyclic limb products: balanced 6-bit limbs at
-// N = 2^16 give 0.144). A group sum of several pairs adds their errors in
+//     err ~ C * rms(d_a) * rms(d_b) * sqrt(N) * sqrt(log2(N/2)) * 2^-p,  C = 7.1
+// with p = 24 (FP32) or 53 (FP64) mantissa bits (calibrated on FP32 negacyclic
+// limb products: balanced 6-bit limbs at N = 2^16 give 0.144). A group sum of
+// several pairs adds their errors in
 // quadrature. The coefficients are signed values of magnitude below 2^B
 // (B = input_bits, or input_bits - 1 after centring non-negative inputs);
 // digits have rms 2^(w-1)/sqrt(3), the top digit 2^tb/sqrt(3) with
 // tb = B - w(k-1) leftover bits. Also returns the typical largest group value
 // (4 sigma) through *mag.
-static double predicted_error(int n_power, int B, int w, int k, bool centred, double* mag)
+static double predicted_error(int n_power, int B, int w, int k, bool centred, double* mag, int prec = 24)
 {
     double r[SPLIT_MAX_LIMBS];
     for (int l = 0; l < k; l++) r[l] = std::ldexp(1.0, w - 1) / std::sqrt(3.0);
@@ -45,20 +47,20 @@ static double predicted_error(int n_power, int B, int w, int k, bool centred, do
     }
     const double sqn = std::sqrt(std::ldexp(1.0, n_power));
     if (mag) *mag = 4.0 * worst * sqn;
-    return 7.1 * worst * sqn * std::sqrt((double)(n_power - 1)) * std::ldexp(1.0, -24);
+    return 7.1 * worst * sqn * std::sqrt((double)(n_power - 1)) * std::ldexp(1.0, -prec);
 }
 
-static bool choose_limbs(int n_power, int input_bits, bool non_negative, int* w_out, int* k_out)
+static bool choose_limbs(int n_power, int input_bits, bool non_negative, int* w_out, int* k_out, int prec = 24)
 {
     // the plan with the fewest limbs whose predicted error is at most 0.2 and
-    // whose group values stay far inside FP32's certifiable range (< 2^21)
+    // whose group values stay far inside the certifiable range (< 2^(p-3))
     const int B = non_negative ? input_bits - 1 : input_bits;
     for (int k = 1; k <= SPLIT_MAX_LIMBS; k++)
     {
         const int w = (B + 1 + k - 1) / k; // k balanced digits of w bits cover 2^B in magnitude
         if (w < 1 || w > 20 || B - w * (k - 1) > w - 1) continue;
         double mag = 0;
-        if (predicted_error(n_power, B, w, k, non_negative, &mag) <= 0.2 && mag < std::ldexp(1.0, 21))
+        if (predicted_error(n_power, B, w, k, non_negative, &mag, prec) <= 0.2 && mag < std::ldexp(1.0, prec - 3))
         {
             *w_out = w;
             *k_out = k;
@@ -68,9 +70,9 @@ static bool choose_limbs(int n_power, int input_bits, bool non_negative, int* w_
     return false;
 }
 
-static long long split_wave(int m, int k, long long batch)
+static long long split_wave(int m, int k, long long batch, size_t cxb = sizeof(cx<float>))
 {
-    const size_t per = (size_t)(4 * k - 1) * ((size_t)1 << m) * sizeof(cx<float>);
+    const size_t per = (size_t)(4 * k - 1) * ((size_t)1 << m) * cxb;
     // Recommended wave: up to 1.25 GiB of limb and group spectra, rounded so
     // that the contiguous passes fill whole waves of the SMs. Measured at
     // N = 2^16 (k = 5, 4.75 MiB per product), batch 256: waves of 23 / 74 / 256
@@ -82,10 +84,10 @@ static long long split_wave(int m, int k, long long batch)
     return w < batch ? w : batch;
 }
 
-// [2k limb spectra | 2k-1 group spectra] of W products (complex float, M each)
-static size_t split_ws_bytes(int m, int k, long long W)
+// [2k limb spectra | 2k-1 group spectra] of W products (complex, M each)
+static size_t split_ws_bytes(int m, int k, long long W, size_t cxb = sizeof(cx<float>))
 {
-    return (size_t)(4 * k - 1) * (size_t)W * ((size_t)1 << m) * sizeof(cx<float>);
+    return (size_t)(4 * k - 1) * (size_t)W * ((size_t)1 << m) * cxb;
 }
 
 
@@ -100,18 +102,22 @@ template <int L> static int launch_inv0(const SplitArgs& a, long long ctas, cuda
     return launch_split(split_inv0<L>, done, a, ctas, s);
 }
 
+// T = float: N = 4 .. 2^22; T = double: N = 4 .. 2^17 (the column-form passes).
+template <typename T>
 static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch, int input_bits,
                      int non_negative, int limb_bits, int num_limbs, const void* tables, void* ws, size_t ws_bytes,
                      unsigned* max_err, cudaStream_t s, bool reset_err = true)
 {
-    if (n_power < 2 || n_power > 22) return GPUFFT_ERROR_INVALID_N_POWER;
+    constexpr bool F32 = sizeof(T) == 4;
+    constexpr int PREC = F32 ? 24 : 53;
+    if (n_power < 2 || n_power > (F32 ? 22 : 17)) return GPUFFT_ERROR_INVALID_N_POWER;
     if (!a || !b || !c || !tables || batch <= 0 || input_bits < 1 || input_bits > 31) return GPUFFT_ERROR_INVALID_VALUE;
     if ((uintptr_t)a % 4 || (uintptr_t)b % 4 || (uintptr_t)c % 8 || (uintptr_t)tables % 8 || (uintptr_t)ws % 8)
         return GPUFFT_ERROR_MISALIGNED;
     int w = limb_bits, k = num_limbs;
     if (w <= 0 || k <= 0)
     {
-        if (!choose_limbs(n_power, input_bits, non_negative != 0, &w, &k)) return GPUFFT_ERROR_INVALID_VALUE;
+        if (!choose_limbs(n_power, input_bits, non_negative != 0, &w, &k, PREC)) return GPUFFT_ERROR_INVALID_VALUE;
     }
     // digits are read from a 64-bit offset value: limbs far above the input
     // range (w (k-1) >= 48) are rejected
@@ -121,8 +127,9 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
 
     const int m = n_power - 1;
     const long long M = 1LL << m;
-    const auto* tab = reinterpret_cast<const cx<float>*>(tables);
-    SplitArgs A{};
+    if ((uintptr_t)tables % sizeof(cx<T>) || (uintptr_t)ws % sizeof(cx<T>)) return GPUFFT_ERROR_MISALIGNED;
+    const auto* tab = reinterpret_cast<const cx<T>*>(tables);
+    SplitArgsT<T> A{};
     A.a = a;
     A.b = b;
     A.roots = tab;
@@ -130,7 +137,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
     A.twist = tab + M;
     A.untwist = tab + 2 * M;
     A.max_err = max_err;
-    A.scale = (float)(1.0 / (double)M);
+    A.scale = (T)(1.0 / (double)M);
     A.w = w;
     A.k = k;
     A.K = non_negative ? (1LL << (input_bits - 1)) : 0;
@@ -149,7 +156,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
 
     // the workspace sets the wave (as many products as it holds, rounded to
     // whole waves of the SMs for the tiled passes)
-    const size_t need1 = split_ws_bytes(m, k, 1);
+    const size_t need1 = split_ws_bytes(m, k, 1, sizeof(cx<T>));
     if (!ws || ws_bytes < need1) return GPUFFT_ERROR_WORKSPACE;
     long long W = (long long)(ws_bytes / need1);
     if (W >= batch)
@@ -170,51 +177,64 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         A.c = c + p0 * 2 * M;
         A.W = wv;
         A.batch = wv;
-        A.spec = reinterpret_cast<cx<float>*>(ws);
+        A.spec = reinterpret_cast<cx<T>*>(ws);
         A.group = A.spec + (size_t)(2 * k) * wv * M;
-        if (m <= EBITS)
+        if constexpr (F32)
         {
-            A.geo = PassGeo{};
-            A.geo.m = m;
-            const long long ctas = (wv * M + ECTA - 1) / ECTA;
-            if (k > SPLIT_SINGLE_MAX_LIMBS) return GPUFFT_ERROR_INVALID_VALUE;
-            int st = (m <= 6) ? launch_split_single_lo(m, A, ctas, s)
-                              : (m <= 9) ? launch_split_single_mid(m, A, ctas, s) : launch_split_single_hi(m, A, ctas, s);
-            if (st) return st;
-            continue;
+            if (m <= EBITS)
+            {
+                A.geo = PassGeo{};
+                A.geo.m = m;
+                const long long ctas = (wv * M + ECTA - 1) / ECTA;
+                if (k > SPLIT_SINGLE_MAX_LIMBS) return GPUFFT_ERROR_INVALID_VALUE;
+                int st = (m <= 6)   ? launch_split_single_lo(m, A, ctas, s)
+                         : (m <= 9) ? launch_split_single_mid(m, A, ctas, s)
+                                    : launch_split_single_hi(m, A, ctas, s);
+                if (st) return st;
+                continue;
+            }
         }
         long long ctas = 0;
-        const int L0 = p.L[0];
+        // rings with one pass (FP64 only here) run a zero-stage column form
+        // (digits, fold, twist) around that single contiguous pass
+        const int L0 = p.np == 1 ? 0 : p.L[0];
+        const int kc = p.np == 1 ? 0 : 1; // the contiguous pass
         // 1. limb extraction + first forward pass (strided), all 2k limbs of a column block
         A.geo = pass_geo(p, 0, m, 0, 2 * wv, &ctas);
+        A.geo.m = m;
         int st;
         if (L0 <= SPLIT_COL_MAX)
         {
             const long long threads = 2 * wv * k * (M >> L0);
             const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
             // int32 rows of both operands in, 2k limb spectra out
-            GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * 8), s, "split_fwd0_col<L%d,k%d>", L0, k);
-            st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
-                split_fwd0_col<LL><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
+            GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * sizeof(cx<T>)), s, "split_fwd0_col<%s,L%d,k%d>",
+                     F32 ? "f32" : "f64", L0, k);
+            st = dispatch_int<0, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+                split_fwd0_col<T, LL><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
                 return check_launch();
             });
         }
-        else
+        else if constexpr (F32)
         {
             st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_fwd0<LL>(A, ctas, s); });
+        }
+        else
+        {
+            return GPUFFT_ERROR_INVALID_N_POWER;
         }
         if (st) return st;
         // 2. last forward pass of the 2k W limb spectra, in place
         {
-            PassArgs<float> q{};
-            q.geo = pass_geo(p, 1, m, 0, 2 * k * wv, &ctas);
+            PassArgs<T> q{};
+            q.geo = pass_geo(p, kc, m, 0, 2 * k * wv, &ctas);
             q.in = A.spec;
             q.out = A.spec;
             q.table = A.roots;
             q.batch = 2 * k * wv;
             q.in_kind = IN_CPX;
             q.out_kind = OUT_CPX;
-            st = launch_pass<float, true>(q, p, 1, ctas, s);
+            st = launch_pass<T, true>(q, p, kc, ctas, s);
             if (st) return st;
         }
         // 3. group sums (a streaming kernel), then the first inverse pass of the
@@ -223,42 +243,49 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
             const long long pts = wv * M;
             {
                 // 2k limb spectra in, 2k-1 group spectra out
-                GF_TRACE(tr, (double)pts * 8 * (4 * k - 1), s, "split_groups<k%d>", k);
+                GF_TRACE(tr, (double)pts * sizeof(cx<T>) * (4 * k - 1), s, "split_groups<%s,k%d>",
+                         F32 ? "f32" : "f64", k);
                 st = dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
-                    split_groups<KK><<<(unsigned)((pts + 255) / 256), 256, 0, s>>>(A);
+                    split_groups<T, KK><<<(unsigned)((pts + 255) / 256), 256, 0, s>>>(A);
                     return check_launch();
                 });
             }
             if (st) return st;
-            PassArgs<float> q{};
-            q.geo = pass_geo(p, 1, m, 0, (2 * k - 1) * wv, &ctas);
+            PassArgs<T> q{};
+            q.geo = pass_geo(p, kc, m, 0, (2 * k - 1) * wv, &ctas);
             q.in = A.group;
             q.out = A.group;
             q.table = A.inv_roots;
             q.batch = (2 * k - 1) * wv;
             q.in_kind = IN_CPX;
             q.out_kind = OUT_CPX;
-            st = launch_pass<float, false>(q, p, 1, ctas, s);
+            st = launch_pass<T, false>(q, p, kc, ctas, s);
             if (st) return st;
         }
         // 4. last inverse pass of every group (strided), rounding, int64 recombination
         A.geo = pass_geo(p, 0, m, 0, wv, &ctas);
+        A.geo.m = m;
         if (L0 <= SPLIT_COL_MAX)
         {
             const long long threads = wv * (M >> L0);
             const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
             // 2k-1 group spectra in, int64 rows out
-            GF_TRACE(tr, (double)wv * M * ((2 * k - 1) * 8 + 2 * 8), s, "split_inv0_col<L%d,k%d>", L0, k);
-            st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+            GF_TRACE(tr, (double)wv * M * ((2 * k - 1) * sizeof(cx<T>) + 2 * 8), s, "split_inv0_col<%s,L%d,k%d>",
+                     F32 ? "f32" : "f64", L0, k);
+            st = dispatch_int<0, SPLIT_COL_MAX>(L0, [&]<int LL>() {
                 return dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
-                    split_inv0_col<LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
+                    split_inv0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
                     return check_launch();
                 });
             });
         }
-        else
+        else if constexpr (F32)
         {
             st = dispatch_int<1, 9>(L0, [&]<int LL>() { return launch_inv0<LL>(A, ctas, s); });
+        }
+        else
+        {
+            return GPUFFT_ERROR_INVALID_N_POWER;
         }
         if (st) return st;
     }
@@ -298,7 +325,7 @@ static int split_mul_host(const int32_t* a, const int32_t* b, int64_t* c, int n_
     const size_t sws_bytes = ws_bytes - slots;
     return run_pipeline(a, b, c, batch, ch, in_row, out_row, ws, slots, s,
                         [&](void* da, void* db, void* dc, long long rows, cudaStream_t st) {
-                            return split_mul(static_cast<const int32_t*>(da), static_cast<const int32_t*>(db),
+                            return split_mul<float>(static_cast<const int32_t*>(da), static_cast<const int32_t*>(db),
                                              static_cast<int64_t*>(dc), n_power, (int)rows, input_bits, non_negative,
                                              w, k, tables, sws, sws_bytes, max_err, st, false);
                         });
@@ -327,8 +354,38 @@ extern "C" int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* 
                                                const void* tables, void* workspace, size_t workspace_bytes,
                                                float* max_error, gpufft_stream_t stream)
 {
-    return gfb::split_mul(a, b, c, n_power, batch, input_bits, non_negative, limb_bits, num_limbs, tables, workspace,
+    return gfb::split_mul<float>(a, b, c, n_power, batch, input_bits, non_negative, limb_bits, num_limbs, tables, workspace,
                           workspace_bytes, reinterpret_cast<unsigned*>(max_error), (cudaStream_t)stream);
+}
+
+// FP64 split product: the same chain with double transforms; its error model
+// (2^-53) takes far fewer limbs (two 12-bit limbs for 24-bit coefficients at
+// N = 2^16: 7 transforms per product instead of 19).
+extern "C" int gpufft_split_plan_f64(int n_power, int input_bits, int non_negative, int* limb_bits, int* num_limbs)
+{
+    if (!limb_bits || !num_limbs || input_bits < 1 || input_bits > 31) return GPUFFT_ERROR_INVALID_VALUE;
+    if (n_power < 2 || n_power > 17) return GPUFFT_ERROR_INVALID_N_POWER;
+    return gfb::choose_limbs(n_power, input_bits, non_negative != 0, limb_bits, num_limbs, 53)
+               ? GPUFFT_SUCCESS
+               : GPUFFT_ERROR_INVALID_VALUE;
+}
+
+extern "C" size_t gpufft_negacyclic_mul_split_f64_workspace_bytes(int n_power, int batch, int num_limbs)
+{
+    if (n_power < 2 || n_power > 17 || batch <= 0 || num_limbs < 1 || num_limbs > gfb::SPLIT_MAX_LIMBS) return 0;
+    const int m = n_power - 1;
+    const long long W = gfb::split_wave(m, num_limbs, batch, sizeof(gfb::cx<double>));
+    return gfb::split_ws_bytes(m, num_limbs, W, sizeof(gfb::cx<double>));
+}
+
+extern "C" int gpufft_negacyclic_mul_split_f64(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch,
+                                               int input_bits, int non_negative, int limb_bits, int num_limbs,
+                                               const void* tables, void* workspace, size_t workspace_bytes,
+                                               float* max_error, gpufft_stream_t stream)
+{
+    return gfb::split_mul<double>(a, b, c, n_power, batch, input_bits, non_negative, limb_bits, num_limbs, tables,
+                                  workspace, workspace_bytes, reinterpret_cast<unsigned*>(max_error),
+                                  (cudaStream_t)stream);
 }
 
 extern "C" size_t gpufft_negacyclic_mul_split_f32_host_workspace_bytes(int n_power, int batch, int chunk,
@@ -458,7 +515,7 @@ static int split_batch_execute(SplitBatchPlan* P, const int32_t* a, const int32_
     bool first = true;
     for (const SplitClass& C : P->classes)
     {
-        const int st = split_mul(a + C.off, b + C.off, c + C.off, C.n_power, (int)C.count, P->input_bits,
+        const int st = split_mul<float>(a + C.off, b + C.off, c + C.off, C.n_power, (int)C.count, P->input_bits,
                                  P->non_negative, C.w, C.k, static_cast<cx<float>*>(P->d_tabs) + C.tab_off, P->d_ws,
                                  P->ws_bytes, max_err, s, first);
         if (st) return st;

@@ -54,38 +54,39 @@ __device__ __forceinline__ int split_digit(long long V, int l, int w, int k)
     return (int)((V >> (w * l)) & ((1LL << w) - 1)) - (1 << (w - 1));
 }
 
-struct SplitArgs
+template <typename T> struct SplitArgsT
 {
     const int32_t* a;
     const int32_t* b;
     int64_t* c;
-    cx<float>* spec;  // [2k][W][M] limb spectra (operand-major: a limbs then b limbs)
-    cx<float>* group; // [2k-1][W][M] group spectra
-    const cx<float>* roots;
-    const cx<float>* inv_roots;
-    const cx<float>* twist;
-    const cx<float>* untwist;
+    cx<T>* spec;  // [2k][W][M] limb spectra (operand-major: a limbs then b limbs)
+    cx<T>* group; // [2k-1][W][M] group spectra
+    const cx<T>* roots;
+    const cx<T>* inv_roots;
+    const cx<T>* twist;
+    const cx<T>* untwist;
     unsigned* max_err; // float bits of the largest pre-rounding error (may be null)
-    const cx<float>* uspec; // transform of the all-ones polynomial (table block)
+    const cx<T>* uspec; // transform of the all-ones polynomial (table block)
     long long K;       // centring offset subtracted from every coefficient (0: none)
     long long voff;    // split_digit offset minus K: V = x + voff for a raw coefficient x
     long long uucoef;  // K^2 - K S (mod 2^64): exact int64 u*u correction (uu_term)
     int uq, ur;        // K = 2^(w uq + ur): centring term joins groups s = l + uq, scaled 2^ur
-    float scale;
+    T scale;
     int w, k;
     long long W; // products per wave (stride of the workspace)
     long long batch;
     PassGeo geo;
 };
+using SplitArgs = SplitArgsT<float>;
 
-// Distance of a group value to its nearest integer. Above 2^22 every float is
-// (nearly) an integer and the distance no longer certifies exactness, so such
-// values report 1.0.
-__device__ __forceinline__ float group_error(cx<float> v, float rr, float ri)
+// Distance of a group value to its nearest integer. Above 2^22 (float) or
+// 2^51 (double) every value is (nearly) an integer and the distance no longer
+// certifies exactness, so such values report 1.0.
+template <typename T> __device__ __forceinline__ float group_error(cx<T> v, T rr, T ri)
 {
-    const float lim = 4194304.0f; // 2^22
-    if (fabsf(v.x) >= lim || fabsf(v.y) >= lim) return 1.0f;
-    return fmaxf(fabsf(v.x - rr), fabsf(v.y - ri));
+    const T lim = sizeof(T) == 4 ? (T)4194304.0 : (T)2251799813685248.0; // 2^22, 2^51
+    if (fabs(v.x) >= lim || fabs(v.y) >= lim) return 1.0f;
+    return (float)fmax(fabs(v.x - rr), fabs(v.y - ri));
 }
 
 __device__ __forceinline__ void report_err(unsigned* dst, float e)
@@ -115,7 +116,7 @@ __device__ __forceinline__ void report_err(unsigned* dst, float e)
 // the transform of a zero-mean integer polynomial times u, and the extra
 // sum_{l<k-1} 2^(w (l + q) + r) u u = K S u u (S = sum_{l<k-1} 2^(w l)) is
 // subtracted exactly in int64 with the K^2 term: uucoef = K^2 - K S.
-__device__ __forceinline__ long long uu_term(const SplitArgs& a, long long k, long long N)
+template <typename T> __device__ __forceinline__ long long uu_term(const SplitArgsT<T>& a, long long k, long long N)
 {
     return (long long)((unsigned long long)a.uucoef * (unsigned long long)(2 * k + 2 - N));
 }
@@ -397,7 +398,8 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
 constexpr int SPLIT_COL_MAX = 4;
 constexpr int SPLIT_COL_THREADS = 128;
 
-template <int L0> __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitArgs a)
+template <typename T, int L0>
+__global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitArgsT<T> a)
 {
     constexpr int R = 1 << L0;
     const int m = a.geo.m;
@@ -411,14 +413,14 @@ template <int L0> __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd
     if (bb >= 2 * a.W) return;
     const long long op = bb / a.W, p = bb - op * a.W;
     const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M + c;
-    cx<float> x[R];
+    cx<T> x[R];
 #pragma unroll
     for (int i = 0; i < R; i++)
     {
         const long long V0 = (long long)__ldg(src + i * C) + a.voff;
         const long long V1 = (long long)__ldg(src + i * C + M) + a.voff;
-        const cx<float> f = mk<float>((float)split_digit(V0, l, a.w, a.k), (float)split_digit(V1, l, a.w, a.k));
-        x[i] = cmul<float>(f, ldg<float>(a.twist + c + i * C));
+        const cx<T> f = mk<T>((T)split_digit(V0, l, a.w, a.k), (T)split_digit(V1, l, a.w, a.k));
+        x[i] = cmul<T>(f, ldg<T>(a.twist + c + i * C));
     }
 #pragma unroll
     for (int s = 0; s < L0; s++)
@@ -426,14 +428,15 @@ template <int L0> __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd
         const int h = 1 << (L0 - 1 - s);
 #pragma unroll
         for (int i = 0; i < R; i++)
-            if (!(i & h)) ct_bfly<float>(x[i], x[i + h], ldg<float>(a.roots + (i >> (L0 - s))));
+            if (!(i & h)) ct_bfly<T>(x[i], x[i + h], ldg<T>(a.roots + (i >> (L0 - s))));
     }
-    cx<float>* dst = a.spec + ((op * a.k + l) * a.W + p) * M + c;
+    cx<T>* dst = a.spec + ((op * a.k + l) * a.W + p) * M + c;
 #pragma unroll
     for (int i = 0; i < R; i++) dst[i * C] = x[i];
 }
 
-template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_inv0_col(const SplitArgs a)
+template <typename T, int L0, int K>
+__global__ void __launch_bounds__(SPLIT_COL_THREADS) split_inv0_col(const SplitArgsT<T> a)
 {
     constexpr int R = 1 << L0;
     const int m = a.geo.m;
@@ -445,12 +448,12 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL_THREADS) sp
     // out-of-range threads still reach report_err's warp shuffle
     const bool ok = p0 < a.W;
     const long long p = ok ? p0 : 0;
-    cx<float> un[R];
+    cx<T> un[R];
 #pragma unroll
     for (int i = 0; i < R; i++)
     {
-        const cx<float> u = ldg<float>(a.untwist + c + i * C);
-        un[i] = mk<float>(u.x * a.scale, u.y * a.scale); // scale folded in: exact, scale is 2^-m
+        const cx<T> u = ldg<T>(a.untwist + c + i * C);
+        un[i] = mk<T>(u.x * a.scale, u.y * a.scale); // scale folded in: exact, scale is 2^-m
     }
     long long acc_lo[R], acc_hi[R];
 #pragma unroll
@@ -459,8 +462,8 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL_THREADS) sp
 #pragma unroll
     for (int s = 0; s < 2 * K - 1; s++)
     {
-        const cx<float>* src = a.group + ((long long)s * a.W + p) * M + c;
-        cx<float> x[R];
+        const cx<T>* src = a.group + ((long long)s * a.W + p) * M + c;
+        cx<T> x[R];
 #pragma unroll
         for (int i = 0; i < R; i++) x[i] = __ldcs(src + i * C);
 #pragma unroll
@@ -469,14 +472,14 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL_THREADS) sp
             const int h = 1 << (L0 - 1 - st);
 #pragma unroll
             for (int i = 0; i < R; i++)
-                if (!(i & h)) gs_bfly<float>(x[i], x[i + h], ldg<float>(a.inv_roots + (i >> (L0 - st))));
+                if (!(i & h)) gs_bfly<T>(x[i], x[i + h], ldg<T>(a.inv_roots + (i >> (L0 - st))));
         }
         const int sh = a.w * s;
 #pragma unroll
         for (int i = 0; i < R; i++)
         {
-            const cx<float> v = cmul<float>(x[i], un[i]);
-            const float rr = rintf(v.x), ri = rintf(v.y);
+            const cx<T> v = cmul<T>(x[i], un[i]);
+            const T rr = rint(v.x), ri = rint(v.y);
             err = fmaxf(err, group_error(v, rr, ri));
             acc_lo[i] += (long long)((unsigned long long)(long long)rr << sh);
             acc_hi[i] += (long long)((unsigned long long)(long long)ri << sh);
@@ -502,35 +505,35 @@ constexpr int SPLIT_SINGLE_MAX_LIMBS = 6; // limb counts compiled for rings N <=
 //     G_s[p][j] = sum_{i+l=s} A_i[p][j] B_l[p][j]  (+ 2^ur (A_l + B_l) U[j] for s = l + uq)
 // from the limb spectra [2K][W][M] into the group spectra [2K-1][W][M]. All 2K
 // loads of a point are independent and coalesced across the warp.
-template <int K> __global__ void __launch_bounds__(256) split_groups(const SplitArgs a)
+template <typename T, int K> __global__ void __launch_bounds__(256) split_groups(const SplitArgsT<T> a)
 {
     const long long M = 1LL << a.geo.m;
     const long long n = a.W * M;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
     const long long j = idx & (M - 1);
-    cx<float> v[2 * K];
+    cx<T> v[2 * K];
 #pragma unroll
     for (int t = 0; t < 2 * K; t++) v[t] = __ldcs(a.spec + t * n + idx);
-    cx<float> u = mk<float>(0.f, 0.f);
-    if (a.K) u = ldg<float>(a.uspec + j);
-    const float uscale = (float)(1 << a.ur);
+    cx<T> u = mk<T>(T(0), T(0));
+    if (a.K) u = ldg<T>(a.uspec + j);
+    const T uscale = (T)(1 << a.ur);
 #pragma unroll
     for (int s = 0; s < 2 * K - 1; s++)
     {
-        cx<float> acc = mk<float>(0.f, 0.f);
+        cx<T> acc = mk<T>(T(0), T(0));
 #pragma unroll
         for (int i = 0; i < K; i++)
-            if (s - i >= 0 && s - i < K) acc = cadd<float>(acc, cmul<float>(v[i], v[K + s - i]));
+            if (s - i >= 0 && s - i < K) acc = cadd<T>(acc, cmul<T>(v[i], v[K + s - i]));
         if (a.K)
         {
 #pragma unroll
             for (int l = 0; l < K; l++)
                 if (l + a.uq == s)
                 {
-                    cx<float> e = cadd<float>(v[l], v[K + l]);
-                    if (l < K - 1) e = cadd<float>(e, u);
-                    acc = cadd<float>(acc, cmul<float>(mk<float>(e.x * uscale, e.y * uscale), u));
+                    cx<T> e = cadd<T>(v[l], v[K + l]);
+                    if (l < K - 1) e = cadd<T>(e, u);
+                    acc = cadd<T>(acc, cmul<T>(mk<T>(e.x * uscale, e.y * uscale), u));
                 }
         }
         a.group[s * n + idx] = acc;

@@ -271,6 +271,17 @@ int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* b, int64_t*
                                     int input_bits, int non_negative, int limb_bits, int num_limbs,
                                     const void* tables, void* workspace, size_t workspace_bytes,
                                     float* max_error, gpufft_stream_t stream);
+/* The same exact product with FP64 transforms, N = 2^2 .. 2^17 (no reference
+ * counterpart). Its limb plan uses the FP64 error model, so it needs far fewer
+ * limbs (two 12-bit limbs for 24-bit coefficients at N = 2^16). `tables` is the
+ * f64 native twiddle block (gpufft_ffnt_make_tables_f64). */
+int gpufft_split_plan_f64(int n_power, int input_bits, int non_negative, int* limb_bits, int* num_limbs);
+size_t gpufft_negacyclic_mul_split_f64_workspace_bytes(int n_power, int batch, int num_limbs);
+int gpufft_negacyclic_mul_split_f64(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch,
+                                    int input_bits, int non_negative, int limb_bits, int num_limbs,
+                                    const void* tables, void* workspace, size_t workspace_bytes,
+                                    float* max_error, gpufft_stream_t stream);
+
 /* Mixed ring sizes, exact (no reference counterpart): the split product over
  * a packed batch of requests of different ring sizes (N = 4 .. 2^22). Requests
  * are grouped by size, class-major with the original order inside a class;

@@ -75,3 +75,36 @@ def test_split_error_margin_uniform_24bit(gf, dev, n_power, batch):
     assert gf.split_plan(n_power, 24, True) == (5, 5)
     _, err = gf.negacyclic_mul_split(a, b, input_bits=24, non_negative=True, return_error=True)
     assert float(err.item()) <= 0.25
+
+
+@pytest.mark.parametrize("n_power,batch,lo,hi", [
+    (2, 5, 0, 1 << 24), (6, 7, -(1 << 15), 1 << 15), (12, 3, 0, 1 << 24), (13, 3, -(1 << 20), 1 << 20),
+    (14, 2, 0, 1 << 24), (16, 4, 0, 1 << 24), (17, 2, -(1 << 15), 1 << 15)])
+def test_split_f64_exact(gf, O, dev, n_power, batch, lo, hi):
+    # the exact product with FP64 transforms: bit-exact against the __int128
+    # schoolbook (sampled coefficients above 2^14), error report far below 0.5
+    rng = np.random.default_rng(7000 + n_power)
+    n = 1 << n_power
+    a = rng.integers(lo, hi, (batch, n)).astype(np.int32)
+    b = rng.integers(lo, hi, (batch, n)).astype(np.int32)
+    c, err = gf.negacyclic_mul_split(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev), return_error=True,
+                                     precision="f64")
+    got = c.cpu().numpy()
+    assert float(err.item()) < 0.01
+    if n_power <= 14:
+        assert np.array_equal(got, exact_rows(O, a, b))
+    else:
+        idx = np.sort(rng.choice(n, 512, replace=False)).astype(np.int32)
+        assert np.array_equal(got[:, idx], exact_rows(O, a, b, idx))
+
+
+def test_split_f64_matches_f32_full_batch(gf, dev):
+    # the headline workload through both exact products: identical int64 results
+    rng = np.random.default_rng(77)
+    n, batch = 1 << 16, 64
+    a = torch.from_numpy(rng.integers(0, 1 << 24, (batch, n)).astype(np.int32)).to(dev)
+    b = torch.from_numpy(rng.integers(0, 1 << 24, (batch, n)).astype(np.int32)).to(dev)
+    assert gf.split_plan(16, 24, True, "f64") == (12, 2)
+    c64 = gf.negacyclic_mul_split(a, b, input_bits=24, non_negative=True, precision="f64")
+    c32 = gf.negacyclic_mul_split(a, b, input_bits=24, non_negative=True, precision="f32")
+    assert torch.equal(c64, c32)
