@@ -79,6 +79,10 @@ def lib() -> ctypes.CDLL:
         L.gpufft_negacyclic_mul_f32.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
         L.gpufft_negacyclic_mul_f64.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
         L.gpufft_negacyclic_mul_f64_noalloc.argtypes = [vp, vp, vp, i, i, vp, vp]
+        L.gpufft_cyclic_mul_workspace_bytes.argtypes = [i, i, i]
+        L.gpufft_cyclic_mul_workspace_bytes.restype = sz
+        L.gpufft_cyclic_mul_f32.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
+        L.gpufft_cyclic_mul_f64.argtypes = [vp, vp, vp, i, i, vp, vp, sz, vp]
         L.gpufft_host_fft_tables_f32.argtypes = [i, vp, vp, vp]
         L.gpufft_host_fft_tables_f64.argtypes = [i, vp, vp, vp]
         L.gpufft_host_ffnt_tables_f32.argtypes = [i, vp, vp, vp, vp]
@@ -295,6 +299,32 @@ def negacyclic_mul(a, b, out=None, tables=None, workspace=None, stream=None):
     f = L.gpufft_negacyclic_mul_f64 if f64 else L.gpufft_negacyclic_mul_f32
     check(f(_ptr(a), _ptr(b), _ptr(out), n_power, batch, _ptr(tables), ws_ptr, ws_len, _stream_handle(stream)),
           "negacyclic_mul")
+    return out
+
+
+def cyclic_mul(a, b, out=None, tables=None, workspace=None, stream=None):
+    """c = a * b mod (X^M - 1) for every row of the (batch, M) complex tensors a, b:
+    the C_C product of GPU_FFT forward + inverse-with-multiplication, fused."""
+    import torch
+    batch, n = a.shape
+    n_power = n.bit_length() - 1
+    if (1 << n_power) != n or b.shape != a.shape or a.dtype != b.dtype or a.dtype not in (torch.complex64,
+                                                                                          torch.complex128):
+        raise GpufftError(ERROR_INVALID_VALUE, "a and b must be (batch, 2^k) complex tensors of one dtype")
+    f64 = a.dtype == torch.complex128
+    if tables is None:
+        tables = ffnt_tables(n_power + 1, "f64" if f64 else "f32", a.device, stream)
+    if out is None:
+        out = torch.empty_like(a)
+    L = lib()
+    need = int(L.gpufft_cyclic_mul_workspace_bytes(n_power, batch, 64 if f64 else 32))
+    if workspace is None and need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=a.device)
+    ws_ptr = workspace.data_ptr() if workspace is not None else None
+    ws_len = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    f = L.gpufft_cyclic_mul_f64 if f64 else L.gpufft_cyclic_mul_f32
+    check(f(_ptr(a), _ptr(b), _ptr(out), n_power, batch, _ptr(tables), ws_ptr, ws_len, _stream_handle(stream)),
+          "cyclic_mul")
     return out
 
 

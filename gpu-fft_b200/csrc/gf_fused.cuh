@@ -21,7 +21,9 @@ template <typename T> struct FusedArgs
     T scale;
     long long batch; // products handled by this launch
     PassGeo geo;
-    int lin; // linear (zero-padded) operands: rows of M reals, x_j = f_j
+    int lin;  // linear (zero-padded) operands: rows of M reals, x_j = f_j
+    int cplx; // cyclic product of complex rows of M (no twist): a, b, c point to
+              // COMPLEX<T> rows, c is scaled, SINGLE only
 };
 
 // Contiguous pass over both operands: all forward stages of the pass on A and
@@ -48,7 +50,12 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
         {
             if (tl.b[r] < a.batch)
             {
-                if (SINGLE)
+                if (SINGLE && a.cplx)
+                {
+                    x[0][r] = ld_stream(reinterpret_cast<const cx<T>*>(a.a) + tl.b[r] * M + tl.j[r]);
+                    x[1][r] = ld_stream(reinterpret_cast<const cx<T>*>(a.b) + tl.b[r] * M + tl.j[r]);
+                }
+                else if (SINGLE)
                 {
                     const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
                     if (a.lin)
@@ -92,7 +99,11 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
     for (int r = 0; r < RPT; r++)
     {
         if (tl.b[r] >= a.batch) continue;
-        if (SINGLE)
+        if (SINGLE && a.cplx)
+        {
+            st_stream(reinterpret_cast<cx<T>*>(a.c) + tl.b[r] * M + tl.j[r], cmul<T>(z[0][r], mk<T>(a.scale, T(0))));
+        }
+        else if (SINGLE)
         {
             const cx<T> v = cmul<T>(cmul<T>(z[0][r], mk<T>(a.scale, T(0))), ldg<T>(a.untwist + tl.j[r]));
             T* pc = a.c + tl.b[r] * 2 * M + tl.j[r];

@@ -17,8 +17,9 @@ enum InKind
     IN_FOLD2 = 4, // IN_FOLD with batch entries [0, split) from `in`, the rest from `in2`
     IN_LIN2 = 5,  // zero-padded linear operand: x_j = f_j (real, rows of M), then twist;
                   // batch entries [0, split) from `in`, the rest from `in2`
-    IN_VJP3 = 6   // batch entries [0, split): IN_FOLD from `in` (rows of 2M);
+    IN_VJP3 = 6,  // batch entries [0, split): IN_FOLD from `in` (rows of 2M);
                   // [split, 2 split): IN_LIN from `in2`; [2 split, 3 split): IN_LIN from `in3`
+    IN_CPX2 = 7   // complex rows of M: batch entries [0, split) from `in`, the rest from `in2`
 };
 enum OutKind
 {
@@ -112,6 +113,11 @@ template <typename T>
 __device__ __forceinline__ cx<T> load_elem(const PassArgs<T>& a, int kind, long long b, long long j)
 {
     const long long M = 1LL << a.geo.m;
+    if (kind == IN_CPX2)
+    {
+        const cx<T>* base = reinterpret_cast<const cx<T>*>(b < a.split ? a.in : a.in2);
+        return ld_stream(base + (b < a.split ? b : b - a.split) * M + j);
+    }
     if (kind == IN_CPX)
     {
         if (a.zero_pad && j >= (M >> 1)) return mk<T>(T(0), T(0));
@@ -452,6 +458,7 @@ static inline int launch_col_pass(const PassArgs<T>& a, cudaStream_t s)
         case IN_FOLD2: return go(col_pass_kernel<T, true, L, IN_FOLD2, OUT_CPX>);
         case IN_LIN2: return go(col_pass_kernel<T, true, L, IN_LIN2, OUT_CPX>);
         case IN_VJP3: return go(col_pass_kernel<T, true, L, IN_VJP3, OUT_CPX>);
+        case IN_CPX2: return go(col_pass_kernel<T, true, L, IN_CPX2, OUT_CPX>);
         default: return -1;
         }
     }

@@ -61,8 +61,10 @@ template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
     }
 }
 
+// Both operands live in registers: double needs 255 per thread (one CTA per
+// SM), float fits 128 (two CTAs per SM, 16 warps).
 template <typename T, int L, bool SINGLE>
-__global__ void __launch_bounds__(NTHR, 1) fused_kernel(const FusedArgs<T> a)
+__global__ void __launch_bounds__(NTHR, sizeof(T) == 4 ? 2 : 1) fused_kernel(const FusedArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     fused_body<T, L, SINGLE>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
@@ -207,6 +209,95 @@ static int negacyclic_mul(const T* a, const T* b, T* c, int n_power, int batch, 
     return GPUFFT_SUCCESS;
 }
 
+// Cyclic product of complex vectors, c = a * b mod (X^M - 1), M = 2^n_power:
+// the C_C product the reference forms with GPU_FFT (forward of both operands,
+// inverse with the product, fft.cu:517-598), fused like the negacyclic
+// product. The transforms are cyclic, so no twist: the roots are the first
+// M/2 entries of the native block of the ring 2M, the same values as
+// FFT<T>(M/2)'s bit-reversed table.
+template <typename T>
+static int cyclic_mul(const cx<T>* a, const cx<T>* b, cx<T>* c, int n_power, int batch, const void* tables, void* ws,
+                      size_t ws_bytes, cudaStream_t s)
+{
+    if (n_power < 1 || n_power > NATIVE_MAX_NPOWER - 1) return GPUFFT_ERROR_INVALID_N_POWER;
+    if (!a || !b || !c || !tables || batch <= 0) return GPUFFT_ERROR_INVALID_VALUE;
+    if ((uintptr_t)a % sizeof(cx<T>) || (uintptr_t)b % sizeof(cx<T>) || (uintptr_t)c % sizeof(cx<T>) ||
+        (uintptr_t)tables % sizeof(cx<T>) || (uintptr_t)ws % sizeof(cx<T>))
+        return GPUFFT_ERROR_MISALIGNED;
+    const int m = n_power;
+    const long long M = 1LL << m;
+    const auto* tab = reinterpret_cast<const cx<T>*>(tables);
+    FusedArgs<T> f{};
+    f.roots = tab;
+    f.inv_roots = tab + M / 2;
+    f.scale = (T)(1.0 / (double)M);
+    f.cplx = 1;
+    if (m <= EBITS)
+    {
+        f.a = reinterpret_cast<const T*>(a);
+        f.b = reinterpret_cast<const T*>(b);
+        f.c = reinterpret_cast<T*>(c);
+        f.batch = batch;
+        f.geo = PassGeo{};
+        f.geo.m = m;
+        const long long ctas = ((long long)batch * M + ECTA - 1) / ECTA;
+        return launch_fused<T, true>(f, ctas, s);
+    }
+    const size_t per = 2 * (size_t)M * sizeof(cx<T>);
+    if (!ws || ws_bytes < per) return GPUFFT_ERROR_WORKSPACE;
+    long long W = (long long)(ws_bytes / per);
+    if (W >= batch)
+        W = batch;
+    else
+        W = round_wave(W, M / ECTA);
+    cx<T>* wsp = reinterpret_cast<cx<T>*>(ws);
+    const Plan p = make_plan(m);
+    if (p.np != 2) return GPUFFT_ERROR_INVALID_N_POWER;
+    for (long long p0 = 0; p0 < batch; p0 += W)
+    {
+        const long long w = (batch - p0) < W ? (batch - p0) : W;
+        {
+            long long ctas = 0;
+            PassArgs<T> k{};
+            k.geo = pass_geo(p, 0, m, 0, 2 * w, &ctas);
+            k.in = a + p0 * M;
+            k.in2 = b + p0 * M;
+            k.split = w;
+            k.out = wsp;
+            k.table = f.roots;
+            k.batch = 2 * w;
+            k.in_kind = IN_CPX2;
+            k.out_kind = OUT_CPX;
+            int st = launch_pass<T, true>(k, p, 0, ctas, s);
+            if (st) return st;
+        }
+        {
+            long long ctas = 0;
+            f.geo = pass_geo(p, 1, m, 0, w, &ctas);
+            f.ws = wsp;
+            f.batch = w;
+            int st = launch_fused<T, false>(f, ctas, s);
+            if (st) return st;
+        }
+        {
+            long long ctas = 0;
+            PassArgs<T> k{};
+            k.geo = pass_geo(p, 0, m, 0, w, &ctas);
+            k.in = wsp;
+            k.out = c + p0 * M;
+            k.table = f.inv_roots;
+            k.scale = mk<T>(f.scale, T(0));
+            k.do_scale = 1;
+            k.batch = w;
+            k.in_kind = IN_CPX;
+            k.out_kind = OUT_CPX;
+            int st = launch_pass<T, false>(k, p, 0, ctas, s);
+            if (st) return st;
+        }
+    }
+    return GPUFFT_SUCCESS;
+}
+
 template <typename T> static int make_tables(int n_power, void* tables, cudaStream_t s)
 {
     if (n_power < NATIVE_MIN_NPOWER || n_power > 25) return GPUFFT_ERROR_INVALID_N_POWER;
@@ -247,6 +338,33 @@ extern "C" size_t gpufft_negacyclic_mul_workspace_bytes(int n_power, int batch, 
     if (m <= gfb::EBITS) return 0;
     const long long w = gfb::wave_products(n_power, batch, cxb);
     return (size_t)w * 2 * ((size_t)1 << m) * cxb;
+}
+
+extern "C" size_t gpufft_cyclic_mul_workspace_bytes(int n_power, int batch, int precision_bits)
+{
+    if (n_power < 1 || n_power > gfb::NATIVE_MAX_NPOWER - 1 || batch <= 0) return 0;
+    if (precision_bits != 32 && precision_bits != 64) return 0;
+    const size_t cxb = precision_bits == 64 ? 16 : 8;
+    if (n_power <= gfb::EBITS) return 0;
+    const long long w = gfb::wave_products(n_power + 1, batch, cxb);
+    return (size_t)w * 2 * ((size_t)1 << n_power) * cxb;
+}
+
+extern "C" int gpufft_cyclic_mul_f32(const void* a, const void* b, void* c, int n_power, int batch,
+                                     const void* tables, void* workspace, size_t workspace_bytes,
+                                     gpufft_stream_t stream)
+{
+    using C = gfb::cx<float>;
+    return gfb::cyclic_mul<float>(static_cast<const C*>(a), static_cast<const C*>(b), static_cast<C*>(c), n_power,
+                                  batch, tables, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+extern "C" int gpufft_cyclic_mul_f64(const void* a, const void* b, void* c, int n_power, int batch,
+                                     const void* tables, void* workspace, size_t workspace_bytes,
+                                     gpufft_stream_t stream)
+{
+    using C = gfb::cx<double>;
+    return gfb::cyclic_mul<double>(static_cast<const C*>(a), static_cast<const C*>(b), static_cast<C*>(c), n_power,
+                                   batch, tables, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 extern "C" int gpufft_negacyclic_mul_f32(const float* a, const float* b, float* c, int n_power, int batch,

@@ -176,6 +176,19 @@ int gpufft_negacyclic_mul_f64_host(const double* a, const double* b, double* c, 
                                    const void* tables, void* workspace, size_t workspace_bytes,
                                    gpufft_stream_t stream);
 
+/* Cyclic product of complex vectors, c[k] = a[k] * b[k] mod (X^M - 1),
+ * M = 2^n_power (n_power in [1, 21]): the C_C product the reference forms with
+ * GPU_FFT (forward of both operands, then the inverse with multiplication and
+ * mod_inverse 1/M; reference fft.cu:517-598, example test_fft_gpu_C_C.cu),
+ * fused into one kernel chain. a, b, c: batch x M COMPLEX<T> (row-major).
+ * `tables` is the native block of the ring 2M (gpufft_ffnt_make_tables_* with
+ * n_power + 1): its roots are FFT<T>(M/2)'s bit-reversed table. */
+size_t gpufft_cyclic_mul_workspace_bytes(int n_power, int batch, int precision_bits);
+int gpufft_cyclic_mul_f32(const void* a, const void* b, void* c, int n_power, int batch, const void* tables,
+                          void* workspace, size_t workspace_bytes, gpufft_stream_t stream);
+int gpufft_cyclic_mul_f64(const void* a, const void* b, void* c, int n_power, int batch, const void* tables,
+                          void* workspace, size_t workspace_bytes, gpufft_stream_t stream);
+
 /* Linear product of real polynomials, the product the reference forms with
  * GPU_FFT R_R on zero-padded inputs (reference fft.cu:600-725, example
  * test_fft_gpu_R_R.cu:153-164): c[k] = a[k] * b[k], a and b rows of

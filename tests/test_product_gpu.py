@@ -90,3 +90,39 @@ def test_f64_linearity_full_size(gf, dev):
     lhs = gf.negacyclic_mul(a1 + a2, b)
     rhs = gf.negacyclic_mul(a1, b) + gf.negacyclic_mul(a2, b)
     assert torch.equal(torch.round(lhs), torch.round(rhs))
+
+
+@pytest.mark.parametrize("n_power,batch,dtype", [
+    (1, 5, torch.complex128), (4, 9, torch.complex64), (10, 7, torch.complex128), (12, 3, torch.complex64),
+    (13, 3, torch.complex128), (16, 5, torch.complex64), (16, 4, torch.complex128), (18, 2, torch.complex128)])
+def test_cyclic_product_vs_fp64_convolution(gf, dev, n_power, batch, dtype):
+    # the native C_C product against an FP64 cyclic convolution (numpy FFT)
+    g = torch.Generator(device="cpu").manual_seed(300 + n_power)
+    M = 1 << n_power
+    a = torch.randn(batch, M, dtype=dtype, generator=g)
+    b = torch.randn(batch, M, dtype=dtype, generator=g)
+    got = gf.cyclic_mul(a.to(dev), b.to(dev)).cpu().numpy().astype(np.complex128)
+    A, B = a.numpy().astype(np.complex128), b.numpy().astype(np.complex128)
+    want = np.fft.ifft(np.fft.fft(A, axis=1) * np.fft.fft(B, axis=1), axis=1)
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < (1e-14 if dtype == torch.complex128 else 2e-6) * max(n_power, 1), err
+
+
+def test_cyclic_product_matches_dropin(gf, O, dev):
+    # identical arithmetic to the reference API's two GPU_FFT calls on the
+    # same tables (FFT<T>(M/2) values): equal within rounding
+    n_power, batch = 14, 6
+    M = 1 << n_power
+    g = torch.Generator(device="cpu").manual_seed(5)
+    a = torch.randn(batch, M, dtype=torch.complex128, generator=g)
+    b = torch.randn(batch, M, dtype=torch.complex128, generator=g)
+    got = gf.cyclic_mul(a.to(dev), b.to(dev)).cpu()
+    roots, inv_roots, _ = gf.host_fft_tables(M // 2, "f64")
+    buf = torch.cat([a.reshape(-1), b.reshape(-1)]).to(dev)
+    L = gf.lib()
+    d_r = torch.from_numpy(np.ascontiguousarray(roots)).to(dev)
+    d_i = torch.from_numpy(np.ascontiguousarray(inv_roots)).to(dev)
+    gf.check(L.gpufft_fft_c2c_f64(buf.data_ptr(), d_r.data_ptr(), n_power, 0, 1, 0, 1.0, 0.0, 2 * batch, 0, None), "f")
+    gf.check(L.gpufft_fft_c2c_f64(buf.data_ptr(), d_i.data_ptr(), n_power, 1, 1, 0, 1.0 / M, 0.0, batch, 1, None), "i")
+    ref = buf[: batch * M].cpu().view(batch, M)
+    assert (torch.linalg.norm(got - ref) / torch.linalg.norm(ref)).item() < 1e-14
