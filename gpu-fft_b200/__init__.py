@@ -69,6 +69,8 @@ def lib() -> ctypes.CDLL:
         L.gpufft_fft_r2r_f64.argtypes = [vp, vp, vp, i, i, i, i, d, d, i, i, vp]
         L.gpufft_ffnt_f32.argtypes = [vp, vp, vp, vp, i, i, f, f, i, i, vp]
         L.gpufft_ffnt_f64.argtypes = [vp, vp, vp, vp, i, i, d, d, i, i, vp]
+        L.gpufft_special_fft_f32.argtypes = [vp, vp, i, i, f, f, i, vp]
+        L.gpufft_special_fft_f64.argtypes = [vp, vp, i, i, d, d, i, vp]
         sz = ctypes.c_size_t
         L.gpufft_ffnt_tables_count.argtypes = [i]
         L.gpufft_ffnt_tables_count.restype = sz
@@ -214,6 +216,18 @@ def GPU_FFT(*args):
         check(st, "GPU_FFT")
         return
     raise TypeError("GPU_FFT takes 5 (C_C) or 6 (R_R) arguments")
+
+
+def GPU_Special_FFT(inout, root_table, cfg, batch):
+    """GPU_Special_FFT (reference fft.cuh:194-197, fft.cu:929-1007): the special FFT
+    of CKKS encoding, in place on batch vectors of 2^n_power complex."""
+    if cfg.n_power <= 10 or cfg.n_power >= 25:  # fft.cu:933-936
+        raise ValueError("Invalid n_power range!")
+    L = lib()
+    f = L.gpufft_special_fft_f64 if _is_f64(inout) else L.gpufft_special_fft_f32
+    mi = complex(cfg.mod_inverse)
+    check(f(_ptr(inout), _ptr(root_table), cfg.n_power, int(cfg.fft_type), mi.real, mi.imag, int(batch),
+            _stream_handle(cfg.stream)), "GPU_Special_FFT")
 
 
 def GPU_FFNT(inout, temp, twist_table, root_table, cfg, batch, multiplication):

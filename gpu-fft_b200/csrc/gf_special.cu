@@ -1,0 +1,200 @@
+// gpufft-b200: GPU_Special_FFT (the reference's "special FFT" for the CKKS
+// canonical embedding, fft.cu:727-1007, launch tables fft.cuh:388-500).
+//
+// The reference's network on vectors of 2^m complex, in place: the span
+// t = 2^p pairs i and i + t (i the lower element of its group of 2t) with the
+// twiddle table[t + (i mod t)] -- indexed by the position inside the group,
+// where the FFT/FFNT stages index by the group. The forward runs the spans
+// 1, 2, ..., 2^(m-1) with Cooley-Tukey butterflies; the inverse runs them
+// back down with Gentleman-Sande butterflies and multiplies every value by
+// cfg.mod_inverse at the end.
+//
+// B200 form: the spans are cut into passes of at most four; a pass is one
+// thread per column (the 2^L points base + k 2^p0 of one lower offset below
+// the pass's first span p0), in registers, with no barrier. Neighbouring
+// threads take neighbouring lower offsets, so passes with p0 >= 5 are
+// coalesced as they stand; the pass of spans 1..8 (p0 = 0), whose columns are
+// 16 consecutive points, stages 2048-point runs through padded shared memory
+// so that its global loads and stores stay coalesced too.
+#include "gf_engine.cuh"
+
+namespace gfb
+{
+
+template <typename T> struct SpecialArgs
+{
+    cx<T>* data;
+    const cx<T>* table;
+    cx<T> scale;
+    long long batch;
+    int m, p0, do_scale;
+};
+
+constexpr int SPECIAL_THREADS = 128;
+
+template <typename T, int L, bool FWD>
+__device__ __forceinline__ void special_network(cx<T> (&x)[1 << L], const SpecialArgs<T>& a, long long lo)
+{
+#pragma unroll
+    for (int q = 0; q < L; q++)
+    {
+        const int s = FWD ? q : L - 1 - q; // span 2^(p0 + s)
+        const int h = 1 << s;
+        const cx<T>* tw = a.table + (1LL << (a.p0 + s)) + lo;
+#pragma unroll
+        for (int k = 0; k < (1 << L); k++)
+        {
+            if (k & h) continue;
+            const cx<T> w = ldg<T>(tw + ((long long)(k & (h - 1)) << a.p0));
+            if (FWD)
+                ct_bfly<T>(x[k], x[k + h], w);
+            else
+                gs_bfly<T>(x[k], x[k + h], w);
+        }
+    }
+    if (a.do_scale)
+    {
+#pragma unroll
+        for (int k = 0; k < (1 << L); k++) x[k] = cmul<T>(x[k], a.scale);
+    }
+}
+
+// A pass of spans 2^p0 .. 2^(p0+L-1) (p0 > 0), one column per thread.
+template <typename T, int L, bool FWD>
+__global__ void __launch_bounds__(SPECIAL_THREADS) special_col_kernel(const SpecialArgs<T> a)
+{
+    constexpr int R = 1 << L;
+    const long long idx = (long long)blockIdx.x * SPECIAL_THREADS + threadIdx.x;
+    const int m = a.m, p0 = a.p0;
+    const long long lo = idx & ((1LL << p0) - 1);
+    const long long rest = idx >> p0;
+    const long long hi = rest & ((1LL << (m - p0 - L)) - 1);
+    const long long b = rest >> (m - p0 - L);
+    if (b >= a.batch) return;
+    cx<T>* p = a.data + (b << m) + (hi << (p0 + L)) + lo;
+    cx<T> x[R];
+#pragma unroll
+    for (int k = 0; k < R; k++) x[k] = p[(long long)k << p0];
+    special_network<T, L, FWD>(x, a, lo);
+#pragma unroll
+    for (int k = 0; k < R; k++) p[(long long)k << p0] = x[k];
+}
+
+// The pass of the smallest spans (p0 = 0): every column is 2^L consecutive
+// points. A CTA moves a run of SPECIAL_THREADS * 2^L points through shared
+// memory (padded one slot per 16 so that the column reads are conflict-free).
+template <typename T, int L, bool FWD>
+__global__ void __launch_bounds__(SPECIAL_THREADS) special_first_kernel(const SpecialArgs<T> a)
+{
+    constexpr int R = 1 << L;
+    constexpr int RUN = SPECIAL_THREADS * R;
+    __shared__ cx<T> sm[RUN + RUN / 16];
+    const int t = threadIdx.x;
+    const long long run0 = (long long)blockIdx.x * RUN; // first point of the run (flat over the batch)
+    // the run lies in one vector or covers whole vectors (both are powers of
+    // two, and a vector holds whole columns); the last run may be partial
+    const long long rem = (a.batch << a.m) - run0;
+    if (rem <= 0) return;
+    cx<T>* g = a.data + run0;
+#pragma unroll
+    for (int k = 0; k < R; k++)
+    {
+        const int e = k * SPECIAL_THREADS + t;
+        sm[e + (e >> 4)] = e < rem ? g[e] : mk<T>(T(0), T(0));
+    }
+    __syncthreads();
+    cx<T> x[R];
+#pragma unroll
+    for (int k = 0; k < R; k++)
+    {
+        const int e = t * R + k;
+        x[k] = sm[e + (e >> 4)];
+    }
+    special_network<T, L, FWD>(x, a, 0);
+#pragma unroll
+    for (int k = 0; k < R; k++)
+    {
+        const int e = t * R + k;
+        sm[e + (e >> 4)] = x[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < R; k++)
+    {
+        const int e = k * SPECIAL_THREADS + t;
+        if (e < rem) g[e] = sm[e + (e >> 4)];
+    }
+}
+
+template <typename T, bool FWD> static int launch_special_pass(const SpecialArgs<T>& a, int L, cudaStream_t s)
+{
+    const long long points = a.batch << a.m;
+    return dispatch_int<1, 4>(L, [&]<int LL>() {
+        GF_TRACE(tr, (double)points * 2 * sizeof(cx<T>), s, "special_%s<%s,%s,L%d,p0=%d>",
+                 a.p0 == 0 ? "first" : "col", sizeof(T) == 4 ? "f32" : "f64", FWD ? "fwd" : "inv", LL, a.p0);
+        if (a.p0 == 0)
+        {
+            constexpr long long RUN = (long long)SPECIAL_THREADS << LL;
+            special_first_kernel<T, LL, FWD><<<(unsigned)((points + RUN - 1) / RUN), SPECIAL_THREADS, 0, s>>>(a);
+        }
+        else
+        {
+            const long long threads = points >> LL;
+            special_col_kernel<T, LL, FWD>
+                <<<(unsigned)((threads + SPECIAL_THREADS - 1) / SPECIAL_THREADS), SPECIAL_THREADS, 0, s>>>(a);
+        }
+        return check_launch();
+    });
+}
+
+template <typename T>
+static int special_fft(cx<T>* inout, const cx<T>* table, int n_power, int fft_type, cx<T> mod_inverse, int batch,
+                       cudaStream_t s)
+{
+    if (n_power < 1 || n_power > 24) return GPUFFT_ERROR_INVALID_N_POWER;
+    if (!inout || !table || batch <= 0 || (fft_type != GPUFFT_FORWARD && fft_type != GPUFFT_INVERSE))
+        return GPUFFT_ERROR_INVALID_VALUE;
+    if ((uintptr_t)inout % sizeof(cx<T>) || (uintptr_t)table % sizeof(cx<T>)) return GPUFFT_ERROR_MISALIGNED;
+    int p0s[8], Ls[8], np = 0;
+    for (int p0 = 0; p0 < n_power; p0 += 4)
+    {
+        p0s[np] = p0;
+        Ls[np] = (n_power - p0) < 4 ? (n_power - p0) : 4;
+        np++;
+    }
+    SpecialArgs<T> a{};
+    a.data = inout;
+    a.table = table;
+    a.batch = batch;
+    a.m = n_power;
+    a.scale = mod_inverse;
+    for (int i = 0; i < np; i++)
+    {
+        const int k = fft_type == GPUFFT_FORWARD ? i : np - 1 - i;
+        a.p0 = p0s[k];
+        a.do_scale = fft_type == GPUFFT_INVERSE && i == np - 1;
+        const int st = fft_type == GPUFFT_FORWARD ? launch_special_pass<T, true>(a, Ls[k], s)
+                                                  : launch_special_pass<T, false>(a, Ls[k], s);
+        if (st) return st;
+    }
+    return GPUFFT_SUCCESS;
+}
+
+} // namespace gfb
+
+extern "C" int gpufft_special_fft_f32(void* inout, const void* table, int n_power, int fft_type, float mod_inverse_re,
+                                      float mod_inverse_im, int batch, gpufft_stream_t stream)
+{
+    using C = gfb::cx<float>;
+    return gfb::special_fft<float>(static_cast<C*>(inout), static_cast<const C*>(table), n_power, fft_type,
+                                   gfb::mk<float>(mod_inverse_re, mod_inverse_im), batch, (cudaStream_t)stream);
+}
+
+extern "C" int gpufft_special_fft_f64(void* inout, const void* table, int n_power, int fft_type,
+                                      double mod_inverse_re, double mod_inverse_im, int batch,
+                                      gpufft_stream_t stream)
+{
+    using C = gfb::cx<double>;
+    return gfb::special_fft<double>(static_cast<C*>(inout), static_cast<const C*>(table), n_power, fft_type,
+                                    gfb::mk<double>(mod_inverse_re, mod_inverse_im), batch, (cudaStream_t)stream);
+}

@@ -129,6 +129,16 @@ inline int ffnt(double* io, COMPLEX<double>* t, COMPLEX<double>* tw, COMPLEX<dou
     return gpufft_ffnt_f64(io, t, tw, r, c.n_power, c.fft_type, c.mod_inverse.real(), c.mod_inverse.imag(), b, m,
                            reinterpret_cast<gpufft_stream_t>(c.stream));
 }
+inline int special(COMPLEX<float>* io, COMPLEX<float>* r, const fft_configuration<float>& c, int b)
+{
+    return gpufft_special_fft_f32(io, r, c.n_power, c.fft_type, c.mod_inverse.real(), c.mod_inverse.imag(), b,
+                                  reinterpret_cast<gpufft_stream_t>(c.stream));
+}
+inline int special(COMPLEX<double>* io, COMPLEX<double>* r, const fft_configuration<double>& c, int b)
+{
+    return gpufft_special_fft_f64(io, r, c.n_power, c.fft_type, c.mod_inverse.real(), c.mod_inverse.imag(), b,
+                                  reinterpret_cast<gpufft_stream_t>(c.stream));
+}
 } // namespace detail
 
 // COMPLEX<T> to COMPLEX<T> (reference fft.cuh:120-124)
@@ -161,6 +171,16 @@ inline void GPU_FFNT(T* device_inout, COMPLEX<T>* device_temp, COMPLEX<T>* twist
     detail::raise_status(
         detail::ffnt(device_inout, device_temp, twist_table, root_of_unity_table, cfg, batch_size, multiplication),
         __FILE__, __LINE__);
+}
+
+// Special FFT for HE encoding (reference fft.cuh:194-197; range check as
+// fft.cu:933-936: n_power in [11, 24])
+template <typename T>
+inline void GPU_Special_FFT(COMPLEX<T>* device_inout, COMPLEX<T>* root_of_unity_table, fft_configuration<T> cfg,
+                            int batch_size)
+{
+    if (cfg.n_power <= 10 || cfg.n_power >= 25) throw std::invalid_argument("Invalid n_power range!");
+    detail::raise_status(detail::special(device_inout, root_of_unity_table, cfg, batch_size), __FILE__, __LINE__);
 }
 
 } // namespace gpufft

@@ -148,6 +148,20 @@ size_t gpufft_ffnt_tables_count(int n_power);
 int gpufft_ffnt_make_tables_f32(int n_power, void* tables, gpufft_stream_t stream);
 int gpufft_ffnt_make_tables_f64(int n_power, void* tables, gpufft_stream_t stream);
 
+/* ------------------------------------------------------------------------ */
+/* GPU_Special_FFT (reference fft.cuh:194-197, fft.cu:929-1007): the special */
+/* FFT of CKKS encoding on batch vectors of 2^n_power complex, in place.     */
+/* The span-t butterfly of the pair (i, i + t) uses table[t + (i mod t)]      */
+/* (the table has 2^n_power entries); FORWARD runs spans 1 .. 2^(n-1) with   */
+/* Cooley-Tukey butterflies, INVERSE runs them back with Gentleman-Sande     */
+/* butterflies and multiplies by mod_inverse. n_power in [1, 24] here (the   */
+/* reference accepts 11..24; the C++ and Python mirrors keep that range).    */
+/* ------------------------------------------------------------------------ */
+int gpufft_special_fft_f32(void* inout, const void* table, int n_power, int fft_type, float mod_inverse_re,
+                           float mod_inverse_im, int batch, gpufft_stream_t stream);
+int gpufft_special_fft_f64(void* inout, const void* table, int n_power, int fft_type, double mod_inverse_re,
+                           double mod_inverse_im, int batch, gpufft_stream_t stream);
+
 /* Workspace for gpufft_negacyclic_mul_* (precision_bits 32 or 64); 0 when the
  * ring needs none (N <= 8192). Passing more lets larger waves run per launch. */
 size_t gpufft_negacyclic_mul_workspace_bytes(int n_power, int batch, int precision_bits);

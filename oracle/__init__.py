@@ -52,6 +52,7 @@ def lib():
             getattr(L, f"orc_gpu_fft_c2c_{sfx}").argtypes = [p, p, _c_int, _c_int, _c_int, p, _c_int, _c_int]
             getattr(L, f"orc_gpu_fft_r2r_{sfx}").argtypes = [p, p, p, _c_int, _c_int, _c_int, p, _c_int, _c_int]
             getattr(L, f"orc_gpu_ffnt_{sfx}").argtypes = [p, p, p, p, _c_int, _c_int, p, _c_int, _c_int]
+            getattr(L, f"orc_gpu_special_fft_{sfx}").argtypes = [p, p, _c_int, _c_int, p, _c_int]
             getattr(L, f"orc_cpu_fft_{sfx}").argtypes = [_c_int, p, p]
             getattr(L, f"orc_cpu_ifft_{sfx}").argtypes = [_c_int, p, p, T]
             getattr(L, f"orc_cpu_ffnt_mult_{sfx}").argtypes = [_c_int, _u64p, _u64p, _u64p, p, p, p, p]
@@ -104,6 +105,8 @@ def ref_gpu():
         R.ref_gpu_ffnt_f32.argtypes = [vp, vp, vp, vp, i, i, f, f, i, i, vp]
         R.ref_gpu_fft_c2c_f64.argtypes = [vp, vp, i, i, i, d, d, i, i, vp]
         R.ref_gpu_fft_r2r_f64.argtypes = [vp, vp, vp, i, i, i, d, d, i, i, vp]
+        R.ref_gpu_special_fft_f64.argtypes = [vp, vp, i, i, d, d, i, vp]
+        R.ref_gpu_special_fft_f32.argtypes = [vp, vp, i, i, f, f, i, vp]
         _REFGPU = R
     return _REFGPU
 
@@ -152,6 +155,18 @@ def gpu_fft_c2c(inout, table, n_power, fft_type, reduction_poly, mod_inverse, ba
     mi = np.array([np.real(mod_inverse), np.imag(mod_inverse)], T)
     getattr(lib(), f"orc_gpu_fft_c2c_{_sfx(T)}")(fv, _as_float_view(table.astype(C), T), n_power, fft_type,
                                                   reduction_poly, mi, batch, int(mult))
+    return buf
+
+
+def gpu_special_fft(inout, table, n_power, fft_type, mod_inverse, batch):
+    """GPU_Special_FFT semantics on the CPU (reference fft.cu:727-1007); returns the
+    updated buffer of batch vectors of 2^n_power complex."""
+    C = inout.dtype
+    T = np.float64 if C == np.complex128 else np.float32
+    buf = np.array(inout, dtype=C, copy=True)
+    mi = np.array([np.real(mod_inverse), np.imag(mod_inverse)], T)
+    getattr(lib(), f"orc_gpu_special_fft_{_sfx(T)}")(buf.view(T), _as_float_view(table.astype(C), T), n_power,
+                                                      fft_type, mi, batch)
     return buf
 
 

@@ -311,6 +311,47 @@ ORC_DEFINE(double, f64, cos, sin, exp)
 ORC_DEFINE(float, f32, cosf, sinf, expf)
 
 /* ------------------------------------------------------------------------- */
+/* GPU_Special_FFT (fft.cu:727-1007, launch tables fft.cuh:388-500): radix-2  */
+/* stages on vectors of 2^n_power complex, in place. The span t = 2^p pairs   */
+/* i and i + t (i the lower element of its group of 2t) and uses             */
+/* table[t + (i mod t)] (the kernels' root[m + (omega & (m - 1))]).           */
+/*   forward: spans 1, 2, ..., 2^(n-1), CooleyTukeyUnit (fft.cuh:69-78);      */
+/*   inverse: spans 2^(n-1), ..., 1, GentlemanSandeUnit (fft.cuh:80-89), then */
+/*            every value times mod_inverse (the last inverse kernel).        */
+/* ------------------------------------------------------------------------- */
+#define ORC_SPECIAL(T, SFX)                                                                   \
+    void orc_gpu_special_fft_##SFX(T* inout, const T* table, int n_power, int fft_type,       \
+                                   const T* mod_inverse, int batch)                          \
+    {                                                                                         \
+        long M = 1L << n_power;                                                               \
+        cx_##SFX sc = cmk_##SFX(mod_inverse[0], mod_inverse[1]);                              \
+        for (int b = 0; b < batch; b++) {                                                     \
+            T* p = inout + 2 * (long)b * M;                                                   \
+            for (int s = 0; s < n_power; s++) {                                               \
+                int e = fft_type == 0 ? s : n_power - 1 - s;                                  \
+                long t = 1L << e;                                                             \
+                for (long base = 0; base < M; base += 2 * t)                                  \
+                    for (long j = 0; j < t; j++) {                                            \
+                        cx_##SFX w = ld_##SFX(table, t + j);                                  \
+                        cx_##SFX u = ld_##SFX(p, base + j), v = ld_##SFX(p, base + j + t);    \
+                        if (fft_type == 0) {                                                  \
+                            cx_##SFX vw = cmul_##SFX(v, w);                                   \
+                            st_##SFX(p, base + j, cadd_##SFX(u, vw));                         \
+                            st_##SFX(p, base + j + t, csub_##SFX(u, vw));                     \
+                        } else {                                                              \
+                            st_##SFX(p, base + j, cadd_##SFX(u, v));                          \
+                            st_##SFX(p, base + j + t, cmul_##SFX(csub_##SFX(u, v), w));       \
+                        }                                                                     \
+                    }                                                                         \
+            }                                                                                 \
+            if (fft_type != 0)                                                                \
+                for (long i = 0; i < M; i++) st_##SFX(p, i, cmul_##SFX(ld_##SFX(p, i), sc));  \
+        }                                                                                     \
+    }
+ORC_SPECIAL(double, f64)
+ORC_SPECIAL(float, f32)
+
+/* ------------------------------------------------------------------------- */
 /* Exact integer products (the builder's schoolbook; 128-bit accumulation).   */
 /* Outputs are split into low/high signed 64-bit halves of the __int128.      */
 /* The reference's own schoolbook (fft_cpu.cu:23-73) reduces mod q; these keep */

@@ -84,6 +84,28 @@ int ref_gpu_fft_c2c_f64(void* inout, void* roots, int n_power, int fft_type, int
     });
 }
 
+int ref_gpu_special_fft_f64(void* inout, void* table, int n_power, int fft_type, double mi_re, double mi_im,
+                            int batch, void* stream)
+{
+    fft_configuration<double> cfg{};
+    cfg.n_power = n_power;
+    cfg.fft_type = fft_type ? INVERSE : FORWARD;
+    cfg.mod_inverse = COMPLEX<double>(mi_re, mi_im);
+    cfg.stream = (cudaStream_t)stream;
+    return guarded([&] { GPU_Special_FFT((COMPLEX<double>*)inout, (COMPLEX<double>*)table, cfg, batch); });
+}
+
+int ref_gpu_special_fft_f32(void* inout, void* table, int n_power, int fft_type, float mi_re, float mi_im, int batch,
+                            void* stream)
+{
+    fft_configuration<float> cfg{};
+    cfg.n_power = n_power;
+    cfg.fft_type = fft_type ? INVERSE : FORWARD;
+    cfg.mod_inverse = COMPLEX<float>(mi_re, mi_im);
+    cfg.stream = (cudaStream_t)stream;
+    return guarded([&] { GPU_Special_FFT((COMPLEX<float>*)inout, (COMPLEX<float>*)table, cfg, batch); });
+}
+
 int ref_gpu_fft_r2r_f64(double* real_inout, void* temp, void* roots, int n_power, int fft_type, int red,
                         double mi_re, double mi_im, int batch, int mult, void* stream)
 {

@@ -155,3 +155,22 @@ def test_balanced_digits_roundtrip(O):
         assert np.all(d[:-1] >= -(1 << (w - 1))) and np.all(d[:-1] < (1 << (w - 1)))
         rec = sum(d[l].astype(np.int64) << (w * l) for l in range(k))
         assert np.array_equal(rec, x)
+
+
+def test_special_fft_restatement_known_answer(O):
+    # GPU_Special_FFT's network (fft.cu:727-1007) with the natural table
+    # t + j -> e^{i pi j / t}: the forward of a bit-reversed vector is the
+    # +sign DFT, and the conjugate table with 1/M inverts it
+    n = 6
+    M = 1 << n
+    tab = np.zeros(M, np.complex128)
+    for e in range(n):
+        t = 1 << e
+        tab[t:2 * t] = np.exp(1j * np.pi * np.arange(t) / t)
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    br = np.array([int(format(i, f"0{n}b")[::-1], 2) for i in range(M)])
+    y = O.gpu_special_fft(x[br].copy(), tab, n, 0, 1.0, 1)
+    assert np.abs(y - M * np.fft.ifft(x)).max() < 1e-12
+    z = O.gpu_special_fft(y, np.conj(tab), n, 1, 1.0 / M, 1)
+    assert np.abs(z - x[br]).max() < 1e-13
