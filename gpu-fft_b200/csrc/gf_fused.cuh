@@ -45,42 +45,59 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
         const Tile<L, false, W0> tl(a.geo, cta, t);
         c.g = tl.g;
         c.vec = tw_vec_ok<T>(a.roots) && tw_vec_ok<T>(a.inv_roots);
-#pragma unroll
-        for (int r = 0; r < RPT; r++)
+        // the variant is uniform: one straight-line loop per variant, so a
+        // thread's loads are issued together
+        const cx<T> zero = mk<T>(T(0), T(0));
+        if (SINGLE && a.cplx)
         {
-            if (tl.b[r] < a.batch)
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
             {
-                if (SINGLE && a.cplx)
-                {
-                    x[0][r] = ld_stream(reinterpret_cast<const cx<T>*>(a.a) + tl.b[r] * M + tl.j[r]);
-                    x[1][r] = ld_stream(reinterpret_cast<const cx<T>*>(a.b) + tl.b[r] * M + tl.j[r]);
-                }
-                else if (SINGLE)
-                {
-                    const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
-                    if (a.lin)
-                    {
-                        x[0][r] = cmul<T>(mk<T>(ld_stream(a.a + tl.b[r] * M + tl.j[r]), T(0)), tw);
-                        x[1][r] = cmul<T>(mk<T>(ld_stream(a.b + tl.b[r] * M + tl.j[r]), T(0)), tw);
-                    }
-                    else
-                    {
-                        const T* pa = a.a + tl.b[r] * 2 * M + tl.j[r];
-                        const T* pb = a.b + tl.b[r] * 2 * M + tl.j[r];
-                        x[0][r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
-                        x[1][r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
-                    }
-                }
-                else
-                {
-                    x[0][r] = a.ws[tl.b[r] * M + tl.j[r]];
-                    x[1][r] = a.ws[(a.batch + tl.b[r]) * M + tl.j[r]];
-                }
+                const bool ok = tl.b[r] < a.batch;
+                x[0][r] = ok ? ld_stream(reinterpret_cast<const cx<T>*>(a.a) + tl.b[r] * M + tl.j[r]) : zero;
+                x[1][r] = ok ? ld_stream(reinterpret_cast<const cx<T>*>(a.b) + tl.b[r] * M + tl.j[r]) : zero;
             }
-            else
+        }
+        else if (SINGLE && a.lin)
+        {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
             {
-                x[0][r] = mk<T>(T(0), T(0));
-                x[1][r] = x[0][r];
+                if (tl.b[r] >= a.batch)
+                {
+                    x[0][r] = x[1][r] = zero;
+                    continue;
+                }
+                const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
+                x[0][r] = cmul<T>(mk<T>(ld_stream(a.a + tl.b[r] * M + tl.j[r]), T(0)), tw);
+                x[1][r] = cmul<T>(mk<T>(ld_stream(a.b + tl.b[r] * M + tl.j[r]), T(0)), tw);
+            }
+        }
+        else if (SINGLE)
+        {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+            {
+                if (tl.b[r] >= a.batch)
+                {
+                    x[0][r] = x[1][r] = zero;
+                    continue;
+                }
+                const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
+                const T* pa = a.a + tl.b[r] * 2 * M + tl.j[r];
+                const T* pb = a.b + tl.b[r] * 2 * M + tl.j[r];
+                x[0][r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
+                x[1][r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+            {
+                const bool ok = tl.b[r] < a.batch;
+                x[0][r] = ok ? a.ws[tl.b[r] * M + tl.j[r]] : zero;
+                x[1][r] = ok ? a.ws[(a.batch + tl.b[r]) * M + tl.j[r]] : zero;
             }
         }
     }
@@ -95,25 +112,34 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
     run_rounds<T, false, 0, L, 1>(z, sm, a.inv_roots, c, t);
 
     const Tile<L, false, WE> tl(a.geo, cta, t);
-#pragma unroll
-    for (int r = 0; r < RPT; r++)
+    const cx<T> sc = mk<T>(a.scale, T(0));
+    if (SINGLE && a.cplx)
     {
-        if (tl.b[r] >= a.batch) continue;
-        if (SINGLE && a.cplx)
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            if (tl.b[r] < a.batch)
+                st_stream(reinterpret_cast<cx<T>*>(a.c) + tl.b[r] * M + tl.j[r], cmul<T>(z[0][r], sc));
+    }
+    else if (SINGLE)
+    {
+        cx<T> u[RPT]; // untwist factors, loaded together
+#pragma unroll
+        for (int r = 0; r < RPT; r++) u[r] = ldg<T>(a.untwist + tl.j[r]);
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
         {
-            st_stream(reinterpret_cast<cx<T>*>(a.c) + tl.b[r] * M + tl.j[r], cmul<T>(z[0][r], mk<T>(a.scale, T(0))));
-        }
-        else if (SINGLE)
-        {
-            const cx<T> v = cmul<T>(cmul<T>(z[0][r], mk<T>(a.scale, T(0))), ldg<T>(a.untwist + tl.j[r]));
+            if (tl.b[r] >= a.batch) continue;
+            const cx<T> v = cmul<T>(cmul<T>(z[0][r], sc), u[r]);
             T* pc = a.c + tl.b[r] * 2 * M + tl.j[r];
             st_stream(pc, v.x);
             st_stream(pc + M, v.y);
         }
-        else
-        {
-            a.ws[tl.b[r] * M + tl.j[r]] = z[0][r];
-        }
+    }
+    else
+    {
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            if (tl.b[r] < a.batch) a.ws[tl.b[r] * M + tl.j[r]] = z[0][r];
     }
 }
 

@@ -198,6 +198,54 @@ __device__ __forceinline__ void store_elem(const PassArgs<T>& a, int kind, long 
     }
 }
 
+// Every register of a tile through one load (store) variant. The variant is
+// uniform over the launch; dispatching it once outside the register loop keeps
+// each variant straight-line, so the 16 loads of a thread are issued together
+// (a switch per element serialises them into 16 memory round trips, which a
+// launch of a few CTAs cannot hide).
+template <typename T, int K, typename TL>
+__device__ __forceinline__ void load_regs(const PassArgs<T>& a, const TL& tl, cx<T> (&x)[RPT])
+{
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+        x[r] = (tl.b[r] < a.batch) ? load_elem<T>(a, K, tl.b[r], tl.j[r]) : mk<T>(T(0), T(0));
+}
+template <typename T, typename TL>
+__device__ __forceinline__ void load_tile(const PassArgs<T>& a, int kind, const TL& tl, cx<T> (&x)[RPT])
+{
+    switch (kind)
+    {
+    case IN_CPX: load_regs<T, IN_CPX>(a, tl, x); break;
+    case IN_REAL: load_regs<T, IN_REAL>(a, tl, x); break;
+    case IN_FOLD: load_regs<T, IN_FOLD>(a, tl, x); break;
+    case IN_PROD: load_regs<T, IN_PROD>(a, tl, x); break;
+    case IN_FOLD2: load_regs<T, IN_FOLD2>(a, tl, x); break;
+    case IN_LIN2: load_regs<T, IN_LIN2>(a, tl, x); break;
+    case IN_VJP3: load_regs<T, IN_VJP3>(a, tl, x); break;
+    case IN_CPX2: load_regs<T, IN_CPX2>(a, tl, x); break;
+    default: break;
+    }
+}
+template <typename T, int K, typename TL>
+__device__ __forceinline__ void store_regs(const PassArgs<T>& a, const TL& tl, const cx<T> (&x)[RPT])
+{
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+        if (tl.b[r] < a.batch) store_elem<T>(a, K, tl.b[r], tl.j[r], x[r]);
+}
+template <typename T, typename TL>
+__device__ __forceinline__ void store_tile(const PassArgs<T>& a, int kind, const TL& tl, const cx<T> (&x)[RPT])
+{
+    switch (kind)
+    {
+    case OUT_CPX: store_regs<T, OUT_CPX>(a, tl, x); break;
+    case OUT_REAL: store_regs<T, OUT_REAL>(a, tl, x); break;
+    case OUT_UNFOLD: store_regs<T, OUT_UNFOLD>(a, tl, x); break;
+    case OUT_RE2: store_regs<T, OUT_RE2>(a, tl, x); break;
+    default: break;
+    }
+}
+
 // Row pointers of one batch entry for the load kinds whose rows are real
 // coefficients (fold pairs f_j, f_{j+M}, or linear rows with zero imaginary
 // part): selected once per CTA when the whole tile lies in one batch entry.
@@ -296,9 +344,7 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
         }
         else
         {
-#pragma unroll
-            for (int r = 0; r < RPT; r++)
-                x[0][r] = (tl.b[r] < a.batch) ? load_elem<T>(a, kind, tl.b[r], tl.j[r]) : mk<T>(T(0), T(0));
+            load_tile<T>(a, kind, tl, x[0]);
         }
     }
     c.s0 = a.geo.s0;
@@ -336,9 +382,7 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
         }
         else
         {
-#pragma unroll
-            for (int r = 0; r < RPT; r++)
-                if (tl.b[r] < a.batch) store_elem<T>(a, kind, tl.b[r], tl.j[r], x[0][r]);
+            store_tile<T>(a, kind, tl, x[0]);
         }
     }
 }

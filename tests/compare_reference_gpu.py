@@ -6,8 +6,9 @@ data and same tables, and print one JSON line per case.
 
 Cases: the reference's benchmark shape (bench_gpu_ffnt_R_R_mult.cu: FFNT
 product, LogN 12..23, batch 1) and the batched workload (N = 2^16, batch 256,
-FP64). "ours_dropin" is the same two-call drop-in API; "ours_fused" is the
-native fused product. CUDA events, 3 warm-ups, median of 20 timed calls.
+FP64); the C_C product through GPU_FFT (batched); GPU_Special_FFT forward +
+inverse. "ours_dropin" is the same drop-in API; "ours_fused" is the native
+fused product. CUDA events, 3 warm-ups, median of 20 timed calls.
 """
 import json
 import os
@@ -74,6 +75,53 @@ def main():
         print(json.dumps({"case": f"FFNT product f64 N=2^{n_power} batch {batch}", "ref_gpu_ms": t_ref,
                           "ours_dropin_ms": t_ours, "ours_fused_ms": t_fused, "speedup_dropin": t_ref / t_ours,
                           "speedup_fused": (t_ref / t_fused) if t_fused else None}), flush=True)
+    more_cases(gf, R, dev)
+
+
+def more_cases(gf, R, dev):
+    """C_C product through GPU_FFT and GPU_Special_FFT (forward + inverse)."""
+    L = gf.lib()
+    for n_power, batch in ((12, 1024), (16, 64), (16, 1), (20, 4)):
+        M = 1 << n_power
+        roots, inv_roots, _ = O.fft_tables(M // 2, "f64")
+        d_r = torch.from_numpy(np.ascontiguousarray(roots)).to(dev)
+        d_i = torch.from_numpy(np.ascontiguousarray(inv_roots)).to(dev)
+        buf = torch.randn(2 * batch * M, dtype=torch.complex128, device=dev)
+
+        def ref_c2c():
+            R.ref_gpu_fft_c2c_f64(buf.data_ptr(), d_r.data_ptr(), n_power, 0, 1, 1.0, 0.0, 2 * batch, 0, None)
+            R.ref_gpu_fft_c2c_f64(buf.data_ptr(), d_i.data_ptr(), n_power, 1, 1, 1.0 / M, 0.0, batch, 1, None)
+
+        def our_c2c():
+            L.gpufft_fft_c2c_f64(buf.data_ptr(), d_r.data_ptr(), n_power, 0, 1, 0, 1.0, 0.0, 2 * batch, 0, None)
+            L.gpufft_fft_c2c_f64(buf.data_ptr(), d_i.data_ptr(), n_power, 1, 1, 0, 1.0 / M, 0.0, batch, 1, None)
+        t_ref = timed(ref_c2c)
+        t_ours = timed(our_c2c)
+        a = buf[: batch * M].view(batch, M).clone()
+        b = buf[batch * M:].view(batch, M).clone()
+        tab = gf.ffnt_tables(n_power + 1, "f64", dev)
+        out = torch.empty_like(a)
+        ws = torch.empty(max(1, int(L.gpufft_cyclic_mul_workspace_bytes(n_power, batch, 64))), dtype=torch.uint8,
+                         device=dev)
+        t_nat = timed(lambda: gf.cyclic_mul(a, b, out=out, tables=tab, workspace=ws))
+        print(json.dumps({"case": f"C_C product f64 N=2^{n_power} batch {batch}", "ref_gpu_ms": t_ref,
+                          "ours_dropin_ms": t_ours, "ours_fused_ms": t_nat, "speedup_dropin": t_ref / t_ours,
+                          "speedup_fused": t_ref / t_nat}), flush=True)
+    for n_power, batch in ((12, 1), (16, 1), (20, 1), (16, 64), (12, 1024)):
+        M = 1 << n_power
+        x = torch.randn(batch * M, dtype=torch.complex128, device=dev)
+        tab = torch.exp(2j * np.pi * torch.rand(M, dtype=torch.float64, device=dev))
+
+        def special(f):
+            def run():
+                f(x.data_ptr(), tab.data_ptr(), n_power, 0, 1.0, 0.0, batch, None)
+                f(x.data_ptr(), tab.data_ptr(), n_power, 1, 1.0 / M, 0.0, batch, None)
+            return run
+        t_ref = timed(special(R.ref_gpu_special_fft_f64))
+        t_ours = timed(special(L.gpufft_special_fft_f64))
+        print(json.dumps({"case": f"GPU_Special_FFT f64 fwd+inv N=2^{n_power} batch {batch}", "ref_gpu_ms": t_ref,
+                          "ours_dropin_ms": t_ours, "ours_fused_ms": None, "speedup_dropin": t_ref / t_ours,
+                          "speedup_fused": None}), flush=True)
 
 
 if __name__ == "__main__":
