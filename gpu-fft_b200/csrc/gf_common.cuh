@@ -30,6 +30,14 @@ template <typename T> __host__ __device__ __forceinline__ cx<T> mk(T r, T i)
 }
 template <typename T> __device__ __forceinline__ cx<T> cadd(cx<T> a, cx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
 template <typename T> __device__ __forceinline__ cx<T> csub(cx<T> a, cx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+// float: one packed instruction for both components (sm_100's paired FP32
+// add / fma; per component they round exactly like the scalar forms, and
+// fma(b, -1, a) rounds a - b once, exactly like the subtraction).
+template <> __device__ __forceinline__ float2 cadd<float>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub<float>(float2 a, float2 b)
+{
+    return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
 // Products with the rounding spelled out (one plain multiply, one fused
 // multiply-add per component) rather than left to the compiler's contraction,
 // which may fuse either product of a*b - c*d and may choose differently in

@@ -205,14 +205,16 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         int st;
         if (L0 <= SPLIT_COL_MAX)
         {
-            const long long threads = 2 * wv * k * (M >> L0);
+            const long long threads = 2 * wv * (M >> L0);
             const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
             // int32 rows of both operands in, 2k limb spectra out
             GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * sizeof(cx<T>)), s, "split_fwd0_col<%s,L%d,k%d>",
                      F32 ? "f32" : "f64", L0, k);
             st = dispatch_int<0, SPLIT_COL_MAX>(L0, [&]<int LL>() {
-                split_fwd0_col<T, LL><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
-                return check_launch();
+                return dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
+                    split_fwd0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
+                    return check_launch();
+                });
             });
         }
         else if constexpr (F32)

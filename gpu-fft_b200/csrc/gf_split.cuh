@@ -398,41 +398,70 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
 constexpr int SPLIT_COL_MAX = 4;
 constexpr int SPLIT_COL_THREADS = 128;
 
-template <typename T, int L0>
+// One thread per column of one operand of one product: the column's 2 x 2^L0
+// coefficients and twist factors are loaded once, and the K limbs are peeled
+// off in turn (d_l = (V mod 2^w) - 2^(w-1), then V >>= w, the same digits as
+// split_digit), each through the column network and stored.
+template <typename T, int L0, int K>
 __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitArgsT<T> a)
 {
     constexpr int R = 1 << L0;
     const int m = a.geo.m;
     const long long M = 1LL << m, C = M >> L0;
     const long long idx = (long long)blockIdx.x * SPLIT_COL_THREADS + threadIdx.x;
-    // thread order: column fastest, then limb, then (operand, product)
+    // thread order: column fastest, then (operand, product)
     const long long c = idx & (C - 1);
-    const long long rest = idx >> (m - L0);
-    const long long bb = rest / a.k;
-    const int l = (int)(rest - bb * a.k);
+    const long long bb = idx >> (m - L0);
     if (bb >= 2 * a.W) return;
-    const long long op = bb / a.W, p = bb - op * a.W;
+    const long long op = bb >= a.W ? 1 : 0, p = bb - op * a.W;
     const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M + c;
-    cx<T> x[R];
+    long long v0[R], v1[R];
+    cx<T> tw[R];
 #pragma unroll
     for (int i = 0; i < R; i++)
     {
-        const long long V0 = (long long)__ldg(src + i * C) + a.voff;
-        const long long V1 = (long long)__ldg(src + i * C + M) + a.voff;
-        const cx<T> f = mk<T>((T)split_digit(V0, l, a.w, a.k), (T)split_digit(V1, l, a.w, a.k));
-        x[i] = cmul<T>(f, ldg<T>(a.twist + c + i * C));
+        v0[i] = (long long)__ldg(src + i * C) + a.voff;
+        v1[i] = (long long)__ldg(src + i * C + M) + a.voff;
+        tw[i] = ldg<T>(a.twist + c + i * C);
     }
+    const int w = a.w;
+    const long long mask = (1LL << w) - 1;
+    const int half = 1 << (w - 1);
+    cx<T>* dst = a.spec + (op * K * a.W + p) * M + c;
 #pragma unroll
-    for (int s = 0; s < L0; s++)
+    for (int l = 0; l < K; l++)
     {
-        const int h = 1 << (L0 - 1 - s);
+        cx<T> x[R];
 #pragma unroll
         for (int i = 0; i < R; i++)
-            if (!(i & h)) ct_bfly<T>(x[i], x[i + h], ldg<T>(a.roots + (i >> (L0 - s))));
-    }
-    cx<T>* dst = a.spec + ((op * a.k + l) * a.W + p) * M + c;
+        {
+            int d0, d1;
+            if (l < K - 1)
+            {
+                d0 = (int)(v0[i] & mask) - half;
+                d1 = (int)(v1[i] & mask) - half;
+                v0[i] >>= w;
+                v1[i] >>= w;
+            }
+            else
+            {
+                d0 = (int)v0[i];
+                d1 = (int)v1[i];
+            }
+            x[i] = cmul<T>(mk<T>((T)d0, (T)d1), tw[i]);
+        }
 #pragma unroll
-    for (int i = 0; i < R; i++) dst[i * C] = x[i];
+        for (int s = 0; s < L0; s++)
+        {
+            const int h = 1 << (L0 - 1 - s);
+#pragma unroll
+            for (int i = 0; i < R; i++)
+                if (!(i & h)) ct_bfly<T>(x[i], x[i + h], ldg<T>(a.roots + (i >> (L0 - s))));
+        }
+        cx<T>* d = dst + (long long)l * a.W * M;
+#pragma unroll
+        for (int i = 0; i < R; i++) d[i * C] = x[i];
+    }
 }
 
 template <typename T, int L0, int K>
@@ -459,13 +488,37 @@ __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_inv0_col(const SplitA
 #pragma unroll
     for (int i = 0; i < R; i++) acc_lo[i] = acc_hi[i] = 0;
     float err = 0.f;
+    // short columns: group s + 1 is loaded while group s is transformed and
+    // rounded (longer ones would spill the second copy)
+    constexpr bool PF = R * sizeof(cx<T>) <= 64;
+    const cx<T>* src = a.group + p * M + c;
+    const long long gstride = a.W * M;
+    cx<T> nx[R];
+    if constexpr (PF)
+    {
+#pragma unroll
+        for (int i = 0; i < R; i++) nx[i] = __ldcs(src + i * C);
+    }
 #pragma unroll
     for (int s = 0; s < 2 * K - 1; s++)
     {
-        const cx<T>* src = a.group + ((long long)s * a.W + p) * M + c;
         cx<T> x[R];
+        if constexpr (PF)
+        {
 #pragma unroll
-        for (int i = 0; i < R; i++) x[i] = __ldcs(src + i * C);
+            for (int i = 0; i < R; i++) x[i] = nx[i];
+            if (s + 1 < 2 * K - 1)
+            {
+#pragma unroll
+                for (int i = 0; i < R; i++) nx[i] = __ldcs(src + (s + 1) * gstride + i * C);
+            }
+        }
+        else
+        {
+            const cx<T>* g = a.group + ((long long)s * a.W + p) * M + c;
+#pragma unroll
+            for (int i = 0; i < R; i++) x[i] = __ldcs(g + i * C);
+        }
 #pragma unroll
         for (int st = L0 - 1; st >= 0; st--)
         {
