@@ -140,6 +140,8 @@ def lib() -> ctypes.CDLL:
         L.gpufft_status_string.restype = ctypes.c_char_p
         L.gpufft_status_string.argtypes = [i]
         L.gpufft_version.restype = i
+        L.gpufft_set_cluster_tiles.argtypes = [i]
+        L.gpufft_set_cluster_tiles.restype = i
         _lib = L
     return _lib
 
@@ -390,6 +392,13 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
 # ---------------------------------------------------------------------------
 # Per-kernel device-time tracing
 # ---------------------------------------------------------------------------
+def set_cluster_tiles(max_tiles: int) -> int:
+    """Contiguous 12-stage passes over at most `max_tiles` 4096-point tiles run
+    as 8-CTA clusters (small batches); 0 disables, a negative value queries.
+    Results are bit-identical either way. Returns the previous limit."""
+    return int(lib().gpufft_set_cluster_tiles(int(max_tiles)))
+
+
 def trace_enable(on: bool = True) -> None:
     """Bracket every library kernel launch with CUDA events (off by default)."""
     check(lib().gpufft_trace_enable(int(bool(on))), "trace_enable")

@@ -3,7 +3,7 @@
 // the native products.
 #pragma once
 
-#include "gf_engine.cuh"
+#include "gf_cluster.cuh"
 
 namespace gfb
 {
@@ -447,6 +447,24 @@ __device__ __forceinline__ void col_pass_body(const PassArgs<T>& a, long long id
     const long long g = r >> lc;
     const long long C = 1LL << lc;
     const long long j0 = (g << (m - s0)) + (r & (C - 1));
+    // every twiddle of the column's stages (2^u at stage s0 + u), and the
+    // untwist factors of an unfolding store, are loaded before the data: one
+    // memory latency instead of one per stage
+    cx<T> w[R - 1];
+#pragma unroll
+    for (int u = 0; u < L; u++)
+    {
+        const cx<T>* tw = a.table + (a.geo.neg ? (1LL << (s0 + u)) : 0LL) + (g << u);
+#pragma unroll
+        for (int h = 0; h < (1 << u); h++) w[(1 << u) - 1 + h] = ldg<T>(tw + h);
+    }
+    constexpr bool UNTW = OK == OUT_UNFOLD || OK == OUT_RE2;
+    cx<T> un[UNTW ? R : 1];
+    if constexpr (UNTW)
+    {
+#pragma unroll
+        for (int i = 0; i < R; i++) un[i] = ldg<T>(a.twist + j0 + i * C);
+    }
     cx<T> x[R];
 #pragma unroll
     for (int i = 0; i < R; i++) x[i] = load_elem<T>(a, IK, b, j0 + i * C);
@@ -455,20 +473,46 @@ __device__ __forceinline__ void col_pass_body(const PassArgs<T>& a, long long id
     {
         const int u = FWD ? k : L - 1 - k; // stage s0 + u
         const int h = 1 << (L - 1 - u);
-        const cx<T>* tw = a.table + (a.geo.neg ? (1LL << (s0 + u)) : 0LL) + (g << u);
 #pragma unroll
         for (int i = 0; i < R; i++)
         {
             if (i & h) continue;
-            const cx<T> w = ldg<T>(tw + (i >> (L - u)));
+            const cx<T> wt = w[(1 << u) - 1 + (i >> (L - u))];
             if (FWD)
-                ct_bfly<T>(x[i], x[i + h], w);
+                ct_bfly<T>(x[i], x[i + h], wt);
             else
-                gs_bfly<T>(x[i], x[i + h], w);
+                gs_bfly<T>(x[i], x[i + h], wt);
         }
     }
+    if constexpr (OK == OUT_UNFOLD)
+    {
+        const long long M = 1LL << m;
+        T* p = reinterpret_cast<T*>(a.out) + b * 2 * M + j0;
 #pragma unroll
-    for (int i = 0; i < R; i++) store_elem<T>(a, OK, b, j0 + i * C, x[i]);
+        for (int i = 0; i < R; i++)
+        {
+            const cx<T> v = cmul<T>(cmul<T>(x[i], a.scale), un[i]);
+            p[i * C] = v.x;
+            p[i * C + M] = v.y;
+        }
+    }
+    else if constexpr (OK == OUT_RE2)
+    {
+        const long long M = 1LL << m;
+        T* base = reinterpret_cast<T*>(b < a.split ? a.out : a.out2);
+        const long long bb = (b < a.split) ? b : b - a.split;
+#pragma unroll
+        for (int i = 0; i < R; i++)
+        {
+            const cx<T> v = cmul<T>(cmul<T>(x[i], a.scale), un[i]);
+            st_stream(base + bb * M + j0 + i * C, v.x);
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < R; i++) store_elem<T>(a, OK, b, j0 + i * C, x[i]);
+    }
 }
 
 template <typename T, bool FWD, int L, int IK, int OK>
@@ -590,7 +634,26 @@ static inline int launch_pass(const PassArgs<T>& a, const Plan& p, int k, long l
     if (ctas > 0x7fffffffLL) return GPUFFT_ERROR_INVALID_VALUE;
     const int L = p.L[k];
     if (k == p.np - 1)
+    {
+        // a contiguous 12-stage pass over few tiles: spread each tile over a cluster
+        const bool ck = FWD ? a.in_kind == IN_CPX : (a.in_kind == IN_CPX || a.in_kind == IN_PROD);
+        if (L == EBITS && a.geo.m > EBITS && ck && a.out_kind == OUT_CPX && !a.zero_pad && cluster_ok(ctas))
+        {
+            ClusterArgs<T> c{};
+            c.in = static_cast<const cx<T>*>(a.in);
+            c.out = static_cast<cx<T>*>(a.out);
+            c.table = a.table;
+            c.inv_table = a.table;
+            c.scale = a.scale;
+            c.prod_off = a.prod_off;
+            c.m = a.geo.m;
+            c.neg = a.geo.neg;
+            c.prod = a.in_kind == IN_PROD;
+            c.do_scale = a.do_scale;
+            return launch_cluster_pass<T, FWD ? CLM_FWD : CLM_INV>(c, ctas, a.batch, s);
+        }
         return dispatch_int<1, EBITS>(L, [&]<int LL>() { return launch_pass_shape<T, FWD, LL, false>(a, ctas, s); });
+    }
     if (L <= COL_MAX_L)
     {
         const int st = dispatch_int<1, COL_MAX_L>(L, [&]<int LL>() { return launch_col_pass<T, FWD, LL>(a, s); });

@@ -90,6 +90,19 @@ template <typename T, bool SINGLE> static int launch_fused(const FusedArgs<T>& a
 {
     if (ctas <= 0) return GPUFFT_SUCCESS;
     if (ctas > 0x7fffffffLL) return GPUFFT_ERROR_INVALID_VALUE;
+    if (!SINGLE && cluster_ok(ctas))
+    {
+        // few tiles: each tile's middle pass on a cluster of CTAs
+        const long long M = 1LL << a.geo.m;
+        ClusterArgs<T> c{};
+        c.in = a.ws;
+        c.in2 = a.ws + a.batch * M;
+        c.out = a.ws;
+        c.table = a.roots;
+        c.inv_table = a.inv_roots;
+        c.m = a.geo.m;
+        return launch_cluster_pass<T, CLM_FUSED>(c, ctas, a.batch, s);
+    }
     if (!SINGLE) return launch_fused_shape<T, EBITS, false>(a, ctas, s);
     return dispatch_int<1, EBITS>(a.geo.m, [&]<int LL>() { return launch_fused_shape<T, LL, true>(a, ctas, s); });
 }

@@ -32,24 +32,39 @@ template <typename T> struct SpecialArgs
 
 constexpr int SPECIAL_THREADS = 128;
 
+// The 2^L - 1 twiddles of a column at lower offset lo: span 2^(p0+s) uses
+// table[2^(p0+s) + lo + (k mod 2^s) 2^p0], stored at w[2^s - 1 + (k mod 2^s)].
+// Loaded before the data so that their latency overlaps the data loads.
+template <typename T, int L>
+__device__ __forceinline__ void special_twiddles(cx<T> (&w)[(1 << L) - 1], const SpecialArgs<T>& a, long long lo)
+{
+#pragma unroll
+    for (int s = 0; s < L; s++)
+    {
+        const cx<T>* tw = a.table + (1LL << (a.p0 + s)) + lo;
+#pragma unroll
+        for (int k = 0; k < (1 << s); k++) w[(1 << s) - 1 + k] = ldg<T>(tw + ((long long)k << a.p0));
+    }
+}
+
 template <typename T, int L, bool FWD>
-__device__ __forceinline__ void special_network(cx<T> (&x)[1 << L], const SpecialArgs<T>& a, long long lo)
+__device__ __forceinline__ void special_network(cx<T> (&x)[1 << L], const cx<T> (&w)[(1 << L) - 1],
+                                                const SpecialArgs<T>& a)
 {
 #pragma unroll
     for (int q = 0; q < L; q++)
     {
         const int s = FWD ? q : L - 1 - q; // span 2^(p0 + s)
         const int h = 1 << s;
-        const cx<T>* tw = a.table + (1LL << (a.p0 + s)) + lo;
 #pragma unroll
         for (int k = 0; k < (1 << L); k++)
         {
             if (k & h) continue;
-            const cx<T> w = ldg<T>(tw + ((long long)(k & (h - 1)) << a.p0));
+            const cx<T> wt = w[h - 1 + (k & (h - 1))];
             if (FWD)
-                ct_bfly<T>(x[k], x[k + h], w);
+                ct_bfly<T>(x[k], x[k + h], wt);
             else
-                gs_bfly<T>(x[k], x[k + h], w);
+                gs_bfly<T>(x[k], x[k + h], wt);
         }
     }
     if (a.do_scale)
@@ -72,10 +87,12 @@ __global__ void __launch_bounds__(SPECIAL_THREADS) special_col_kernel(const Spec
     const long long b = rest >> (m - p0 - L);
     if (b >= a.batch) return;
     cx<T>* p = a.data + (b << m) + (hi << (p0 + L)) + lo;
+    cx<T> w[R - 1];
+    special_twiddles<T, L>(w, a, lo);
     cx<T> x[R];
 #pragma unroll
     for (int k = 0; k < R; k++) x[k] = p[(long long)k << p0];
-    special_network<T, L, FWD>(x, a, lo);
+    special_network<T, L, FWD>(x, w, a);
 #pragma unroll
     for (int k = 0; k < R; k++) p[(long long)k << p0] = x[k];
 }
@@ -95,6 +112,8 @@ __global__ void __launch_bounds__(SPECIAL_THREADS) special_first_kernel(const Sp
     // two, and a vector holds whole columns); the last run may be partial
     const long long rem = (a.batch << a.m) - run0;
     if (rem <= 0) return;
+    cx<T> w[R - 1];
+    special_twiddles<T, L>(w, a, 0);
     cx<T>* g = a.data + run0;
 #pragma unroll
     for (int k = 0; k < R; k++)
@@ -110,7 +129,7 @@ __global__ void __launch_bounds__(SPECIAL_THREADS) special_first_kernel(const Sp
         const int e = t * R + k;
         x[k] = sm[e + (e >> 4)];
     }
-    special_network<T, L, FWD>(x, a, 0);
+    special_network<T, L, FWD>(x, w, a);
 #pragma unroll
     for (int k = 0; k < R; k++)
     {

@@ -14,6 +14,10 @@ thread_local int g_last_cuda_error = 0;
 
 namespace gfb
 {
+
+// Contiguous 12-stage passes over at most this many 4096-point tiles run as
+// thread-block clusters (gf_cluster.cuh); 0 disables them.
+int g_cluster_max_tiles = 64;
 int set_cuda_error(cudaError_t e)
 {
     g_last_cuda_error = (int)e;
@@ -185,3 +189,10 @@ extern "C" const char* gpufft_status_string(int status)
 }
 
 extern "C" int gpufft_version(void) { return 100; }
+
+extern "C" int gpufft_set_cluster_tiles(int max_tiles)
+{
+    const int prev = gfb::g_cluster_max_tiles;
+    if (max_tiles >= 0) gfb::g_cluster_max_tiles = max_tiles;
+    return prev;
+}

@@ -63,6 +63,14 @@ int gpufft_trace_enable(int on);
 int gpufft_trace_collect(int max_rows, char* names, int name_len, double* total_ms, double* alg_bytes,
                          long long* launches, int* rows);
 
+/* Launches whose contiguous 12-stage pass covers at most max_tiles tiles of
+ * 4096 points (small batches: N = 2^13..2^23 with few products) spread each
+ * tile over a cluster of 8 CTAs instead of one CTA; results are bit-identical
+ * either way. max_tiles = 0 disables the cluster form; a negative value only
+ * queries. Returns the previous limit (default 64). Process-wide; not
+ * synchronised with concurrent calls. */
+int gpufft_set_cluster_tiles(int max_tiles);
+
 /* The cudaError_t of the last GPUFFT_ERROR_CUDA raised on this host thread. */
 int gpufft_last_cuda_error(void);
 /* A static, human-readable string for a gpufft_status value. */

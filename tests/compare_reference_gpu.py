@@ -8,7 +8,8 @@ Cases: the reference's benchmark shape (bench_gpu_ffnt_R_R_mult.cu: FFNT
 product, LogN 12..23, batch 1) and the batched workload (N = 2^16, batch 256,
 FP64); the C_C product through GPU_FFT (batched); GPU_Special_FFT forward +
 inverse. "ours_dropin" is the same drop-in API; "ours_fused" is the native
-fused product. CUDA events, 3 warm-ups, median of 20 timed calls.
+fused product through its C ABI entry point (as the other two are called).
+CUDA events, 3 warm-ups, median of 20 timed calls.
 """
 import json
 import os
@@ -71,7 +72,11 @@ def main():
             c = torch.empty_like(a)
             ws = torch.empty(max(1, gf.negacyclic_mul_workspace_bytes(n_power, batch, 64)), dtype=torch.uint8,
                              device=dev)
-            t_fused = timed(lambda: gf.negacyclic_mul(a, b, out=c, tables=ntab, workspace=ws))
+            L = gf.lib()
+            args = (a.data_ptr(), b.data_ptr(), c.data_ptr(), n_power, batch, ntab.data_ptr(), ws.data_ptr(),
+                    ws.numel(), None)
+            # through the C ABI, like the reference and the drop-in calls
+            t_fused = timed(lambda: gf.check(L.gpufft_negacyclic_mul_f64(*args), "negacyclic_mul"))
         print(json.dumps({"case": f"FFNT product f64 N=2^{n_power} batch {batch}", "ref_gpu_ms": t_ref,
                           "ours_dropin_ms": t_ours, "ours_fused_ms": t_fused, "speedup_dropin": t_ref / t_ours,
                           "speedup_fused": (t_ref / t_fused) if t_fused else None}), flush=True)
@@ -103,7 +108,9 @@ def more_cases(gf, R, dev):
         out = torch.empty_like(a)
         ws = torch.empty(max(1, int(L.gpufft_cyclic_mul_workspace_bytes(n_power, batch, 64))), dtype=torch.uint8,
                          device=dev)
-        t_nat = timed(lambda: gf.cyclic_mul(a, b, out=out, tables=tab, workspace=ws))
+        cargs = (a.data_ptr(), b.data_ptr(), out.data_ptr(), n_power, batch, tab.data_ptr(), ws.data_ptr(),
+                 ws.numel(), None)
+        t_nat = timed(lambda: gf.check(L.gpufft_cyclic_mul_f64(*cargs), "cyclic_mul"))
         print(json.dumps({"case": f"C_C product f64 N=2^{n_power} batch {batch}", "ref_gpu_ms": t_ref,
                           "ours_dropin_ms": t_ours, "ours_fused_ms": t_nat, "speedup_dropin": t_ref / t_ours,
                           "speedup_fused": t_ref / t_nat}), flush=True)
