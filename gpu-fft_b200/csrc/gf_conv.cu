@@ -58,7 +58,7 @@ template <int L, bool SINGLE> __global__ void __launch_bounds__(NTHR, 1) vjp_ker
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            const long long bb = tl.b[r], j = tl.j[r];
+            const long long bb = tl.b(r), j = tl.j(r);
             if (bb >= a.batch)
             {
                 x[0][r] = x[1][r] = x[2][r] = mk<float>(0.f, 0.f);
@@ -96,7 +96,7 @@ template <int L, bool SINGLE> __global__ void __launch_bounds__(NTHR, 1) vjp_ker
 #pragma unroll
     for (int r = 0; r < RPT; r++)
     {
-        const long long bb = te.b[r], j = te.j[r];
+        const long long bb = te.b(r), j = te.j(r);
         if (bb >= a.batch) continue;
         if (SINGLE)
         {

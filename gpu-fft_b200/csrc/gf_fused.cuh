@@ -53,9 +53,9 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
 #pragma unroll
             for (int r = 0; r < RPT; r++)
             {
-                const bool ok = tl.b[r] < a.batch;
-                x[0][r] = ok ? ld_stream(reinterpret_cast<const cx<T>*>(a.a) + tl.b[r] * M + tl.j[r]) : zero;
-                x[1][r] = ok ? ld_stream(reinterpret_cast<const cx<T>*>(a.b) + tl.b[r] * M + tl.j[r]) : zero;
+                const bool ok = tl.b(r) < a.batch;
+                x[0][r] = ok ? ld_stream(reinterpret_cast<const cx<T>*>(a.a) + tl.b(r) * M + tl.j(r)) : zero;
+                x[1][r] = ok ? ld_stream(reinterpret_cast<const cx<T>*>(a.b) + tl.b(r) * M + tl.j(r)) : zero;
             }
         }
         else if (SINGLE && a.lin)
@@ -63,14 +63,14 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
 #pragma unroll
             for (int r = 0; r < RPT; r++)
             {
-                if (tl.b[r] >= a.batch)
+                if (tl.b(r) >= a.batch)
                 {
                     x[0][r] = x[1][r] = zero;
                     continue;
                 }
-                const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
-                x[0][r] = cmul<T>(mk<T>(ld_stream(a.a + tl.b[r] * M + tl.j[r]), T(0)), tw);
-                x[1][r] = cmul<T>(mk<T>(ld_stream(a.b + tl.b[r] * M + tl.j[r]), T(0)), tw);
+                const cx<T> tw = ldg<T>(a.twist + tl.j(r));
+                x[0][r] = cmul<T>(mk<T>(ld_stream(a.a + tl.b(r) * M + tl.j(r)), T(0)), tw);
+                x[1][r] = cmul<T>(mk<T>(ld_stream(a.b + tl.b(r) * M + tl.j(r)), T(0)), tw);
             }
         }
         else if (SINGLE)
@@ -78,26 +78,29 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
 #pragma unroll
             for (int r = 0; r < RPT; r++)
             {
-                if (tl.b[r] >= a.batch)
+                if (tl.b(r) >= a.batch)
                 {
                     x[0][r] = x[1][r] = zero;
                     continue;
                 }
-                const cx<T> tw = ldg<T>(a.twist + tl.j[r]);
-                const T* pa = a.a + tl.b[r] * 2 * M + tl.j[r];
-                const T* pb = a.b + tl.b[r] * 2 * M + tl.j[r];
+                const cx<T> tw = ldg<T>(a.twist + tl.j(r));
+                const T* pa = a.a + tl.b(r) * 2 * M + tl.j(r);
+                const T* pb = a.b + tl.b(r) * 2 * M + tl.j(r);
                 x[0][r] = cmul<T>(mk<T>(ld_stream(pa), ld_stream(pa + M)), tw);
                 x[1][r] = cmul<T>(mk<T>(ld_stream(pb), ld_stream(pb + M)), tw);
             }
         }
         else
         {
+            // the middle pass (M >= 4096): the tile lies in one product
+            const bool ok = tl.b(0) < a.batch;
+            const cx<T>* pa = a.ws + tl.f0;
+            const cx<T>* pb = pa + a.batch * M;
 #pragma unroll
             for (int r = 0; r < RPT; r++)
             {
-                const bool ok = tl.b[r] < a.batch;
-                x[0][r] = ok ? a.ws[tl.b[r] * M + tl.j[r]] : zero;
-                x[1][r] = ok ? a.ws[(a.batch + tl.b[r]) * M + tl.j[r]] : zero;
+                x[0][r] = ok ? pa[tl.df(r)] : zero;
+                x[1][r] = ok ? pb[tl.df(r)] : zero;
             }
         }
     }
@@ -117,29 +120,29 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T>& a, long long cta,
     {
 #pragma unroll
         for (int r = 0; r < RPT; r++)
-            if (tl.b[r] < a.batch)
-                st_stream(reinterpret_cast<cx<T>*>(a.c) + tl.b[r] * M + tl.j[r], cmul<T>(z[0][r], sc));
+            if (tl.b(r) < a.batch)
+                st_stream(reinterpret_cast<cx<T>*>(a.c) + tl.b(r) * M + tl.j(r), cmul<T>(z[0][r], sc));
     }
     else if (SINGLE)
     {
         cx<T> u[RPT]; // untwist factors, loaded together
 #pragma unroll
-        for (int r = 0; r < RPT; r++) u[r] = ldg<T>(a.untwist + tl.j[r]);
+        for (int r = 0; r < RPT; r++) u[r] = ldg<T>(a.untwist + tl.j(r));
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            if (tl.b[r] >= a.batch) continue;
+            if (tl.b(r) >= a.batch) continue;
             const cx<T> v = cmul<T>(cmul<T>(z[0][r], sc), u[r]);
-            T* pc = a.c + tl.b[r] * 2 * M + tl.j[r];
+            T* pc = a.c + tl.b(r) * 2 * M + tl.j(r);
             st_stream(pc, v.x);
             st_stream(pc + M, v.y);
         }
     }
-    else
+    else if (tl.b(0) < a.batch)
     {
+        cx<T>* pz = a.ws + tl.f0;
 #pragma unroll
-        for (int r = 0; r < RPT; r++)
-            if (tl.b[r] < a.batch) a.ws[tl.b[r] * M + tl.j[r]] = z[0][r];
+        for (int r = 0; r < RPT; r++) pz[tl.df(r)] = z[0][r];
     }
 }
 

@@ -59,19 +59,24 @@ template <typename T> struct PassArgs
     int do_scale; // last inverse pass: multiply by scale
 };
 
-// Where the 16 registers of thread t (window W) live: batch entry b[r] and
-// transform index j[r] of every register, for a CTA `cta` of a pass with L
-// stages, strided (columns of the pass share a CTA) or contiguous.
+// Where the 16 registers of thread t (window W) live, for a CTA `cta` of a
+// pass with L stages, strided (columns of the pass share a CTA) or contiguous:
+// register r holds the point with flat index f0 + df(r) = b M + j (batch entry
+// b, transform index j). df(r) is a compile-time constant after unrolling
+// (contiguous: r << W; strided: one shift by the pass's stride), so loads and
+// stores of a tile address a base pointer plus constant offsets; b(r) and
+// j(r) are derived on demand for the variants that need them.
 template <int L, bool STRIDED, int W> struct Tile
 {
-    long long b[RPT];
-    long long j[RPT];
-    long long g; // stage-s0 group (uniform over the CTA)
+    long long g;  // stage-s0 group (uniform over the CTA)
+    long long f0; // flat index of register 0
+    int m;        // log2 transform length
+    int sl;       // strided: log2 stride of the pass's q bits
 
     __device__ __forceinline__ Tile(const PassGeo& G, long long cta, int t)
     {
         const int eb = e_base<W>(t);
-        const long long M = 1LL << G.m;
+        m = G.m;
         if constexpr (STRIDED)
         {
             constexpr int CL = EBITS - L; // log2 columns per CTA
@@ -80,33 +85,34 @@ template <int L, bool STRIDED, int W> struct Tile
             const long long rem = cta & ((1LL << (G.m - EBITS)) - 1);
             g = rem >> lgcpb;
             const long long cblk = rem & ((1LL << lgcpb) - 1);
-            const int sl = G.m - G.s0 - L; // log2 stride S
-            const long long j0 = (g << (G.m - G.s0)) + (cblk << CL) + (eb & ((1 << CL) - 1)) +
-                                 ((long long)(eb >> CL) << sl);
-#pragma unroll
-            for (int r = 0; r < RPT; r++)
-            {
-                // register bits r<<W split into column (below CL) and q (above) parts
-                const int e_r = r << W;
-                const int cpart = e_r & ((1 << CL) - 1);
-                const int qpart = e_r >> CL;
-                b[r] = bb;
-                j[r] = j0 + cpart + ((long long)qpart << sl);
-            }
+            sl = G.m - G.s0 - L; // log2 stride S
+            f0 = (bb << G.m) + (g << (G.m - G.s0)) + (cblk << CL) + (eb & ((1 << CL) - 1)) +
+                 ((long long)(eb >> CL) << sl);
         }
         else
         {
-            const long long gi0 = cta * ECTA + eb;
+            sl = 0;
+            f0 = cta * ECTA + eb;
             g = ((cta * ECTA) >> L) & ((1LL << G.s0) - 1);
-#pragma unroll
-            for (int r = 0; r < RPT; r++)
-            {
-                const long long gi = gi0 + (r << W);
-                b[r] = gi >> G.m;
-                j[r] = gi & (M - 1);
-            }
         }
     }
+    // register bits r << W split into column (below CL) and q (above) parts
+    __device__ __forceinline__ long long df(int r) const
+    {
+        const int e_r = r << W;
+        if constexpr (STRIDED)
+        {
+            constexpr int CL = EBITS - L;
+            return (long long)(e_r & ((1 << CL) - 1)) + ((long long)(e_r >> CL) << sl);
+        }
+        else
+        {
+            return (long long)e_r;
+        }
+    }
+    __device__ __forceinline__ long long flat(int r) const { return f0 + df(r); }
+    __device__ __forceinline__ long long b(int r) const { return flat(r) >> m; }
+    __device__ __forceinline__ long long j(int r) const { return flat(r) & ((1LL << m) - 1); }
 };
 
 template <typename T>
@@ -208,7 +214,7 @@ __device__ __forceinline__ void load_regs(const PassArgs<T>& a, const TL& tl, cx
 {
 #pragma unroll
     for (int r = 0; r < RPT; r++)
-        x[r] = (tl.b[r] < a.batch) ? load_elem<T>(a, K, tl.b[r], tl.j[r]) : mk<T>(T(0), T(0));
+        x[r] = (tl.b(r) < a.batch) ? load_elem<T>(a, K, tl.b(r), tl.j(r)) : mk<T>(T(0), T(0));
 }
 template <typename T, typename TL>
 __device__ __forceinline__ void load_tile(const PassArgs<T>& a, int kind, const TL& tl, cx<T> (&x)[RPT])
@@ -231,7 +237,7 @@ __device__ __forceinline__ void store_regs(const PassArgs<T>& a, const TL& tl, c
 {
 #pragma unroll
     for (int r = 0; r < RPT; r++)
-        if (tl.b[r] < a.batch) store_elem<T>(a, K, tl.b[r], tl.j[r], x[r]);
+        if (tl.b(r) < a.batch) store_elem<T>(a, K, tl.b(r), tl.j(r), x[r]);
 }
 template <typename T, typename TL>
 __device__ __forceinline__ void store_tile(const PassArgs<T>& a, int kind, const TL& tl, const cx<T> (&x)[RPT])
@@ -317,30 +323,34 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
         c.g = tl.g;
         const int kind = a.in_kind;
         const bool real_rows_kind = kind == IN_FOLD || kind == IN_FOLD2 || kind == IN_LIN2 || kind == IN_VJP3;
-        if (one_entry && real_rows_kind && tl.b[0] < a.batch)
+        if (one_entry && real_rows_kind && tl.b(0) < a.batch)
         {
             // straight-line loads: every address is row + j
-            const RealRows<T> rr = real_rows<T>(a, kind, tl.b[0]);
+            const RealRows<T> rr = real_rows<T>(a, kind, tl.b(0));
+            const long long j0 = tl.j(0);
+            const T* pre = rr.re + j0;
+            const cx<T>* ptw = a.twist + j0;
             T re[RPT], im[RPT];
             cx<T> tw[RPT];
 #pragma unroll
             for (int r = 0; r < RPT; r++)
             {
-                re[r] = ld_stream(rr.re + tl.j[r]);
-                im[r] = (rr.im_off >= 0) ? ld_stream(rr.re + rr.im_off + tl.j[r]) : T(0);
-                tw[r] = ldg<T>(a.twist + tl.j[r]);
+                re[r] = ld_stream(pre + tl.df(r));
+                im[r] = (rr.im_off >= 0) ? ld_stream(pre + rr.im_off + tl.df(r)) : T(0);
+                tw[r] = ldg<T>(ptw + tl.df(r));
             }
 #pragma unroll
             for (int r = 0; r < RPT; r++) x[0][r] = cmul<T>(mk<T>(re[r], im[r]), tw[r]);
         }
-        else if (one_entry && kind == IN_CPX && tl.b[0] < a.batch)
+        else if (one_entry && kind == IN_CPX && tl.b(0) < a.batch)
         {
             const long long M = 1LL << a.geo.m;
-            const cx<T>* row = reinterpret_cast<const cx<T>*>(a.in) + tl.b[0] * M;
+            const cx<T>* p = reinterpret_cast<const cx<T>*>(a.in) + tl.f0;
             const bool zp = a.zero_pad != 0;
+            const long long jz = (M >> 1) - tl.j(0); // j(r) >= M/2 <=> df(r) >= jz
 #pragma unroll
             for (int r = 0; r < RPT; r++)
-                x[0][r] = (zp && tl.j[r] >= (M >> 1)) ? mk<T>(T(0), T(0)) : row[tl.j[r]];
+                x[0][r] = (zp && tl.df(r) >= jz) ? mk<T>(T(0), T(0)) : p[tl.df(r)];
         }
         else
         {
@@ -356,28 +366,30 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
     {
         const Tile<L, STRIDED, WOUT> tl(a.geo, cta, t);
         const int kind = a.out_kind;
-        if (one_entry && tl.b[0] < a.batch && (kind == OUT_UNFOLD || kind == OUT_CPX))
+        if (one_entry && tl.b(0) < a.batch && (kind == OUT_UNFOLD || kind == OUT_CPX))
         {
             const long long M = 1LL << a.geo.m;
             if (kind == OUT_UNFOLD)
             {
-                T* row = reinterpret_cast<T*>(a.out) + tl.b[0] * 2 * M;
+                const long long j0 = tl.j(0);
+                T* row = reinterpret_cast<T*>(a.out) + tl.b(0) * 2 * M + j0;
+                const cx<T>* ptw = a.twist + j0;
                 cx<T> u[RPT];
 #pragma unroll
-                for (int r = 0; r < RPT; r++) u[r] = ldg<T>(a.twist + tl.j[r]);
+                for (int r = 0; r < RPT; r++) u[r] = ldg<T>(ptw + tl.df(r));
 #pragma unroll
                 for (int r = 0; r < RPT; r++)
                 {
                     const cx<T> v = cmul<T>(cmul<T>(x[0][r], a.scale), u[r]);
-                    st_stream(row + tl.j[r], v.x);
-                    st_stream(row + M + tl.j[r], v.y);
+                    st_stream(row + tl.df(r), v.x);
+                    st_stream(row + M + tl.df(r), v.y);
                 }
             }
             else
             {
-                cx<T>* row = reinterpret_cast<cx<T>*>(a.out) + tl.b[0] * M;
+                cx<T>* p = reinterpret_cast<cx<T>*>(a.out) + tl.f0;
 #pragma unroll
-                for (int r = 0; r < RPT; r++) row[tl.j[r]] = a.do_scale ? cmul<T>(x[0][r], a.scale) : x[0][r];
+                for (int r = 0; r < RPT; r++) p[tl.df(r)] = a.do_scale ? cmul<T>(x[0][r], a.scale) : x[0][r];
             }
         }
         else

@@ -137,14 +137,14 @@ template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const Spl
 
     // the raw coefficients (fold pair j, j+M) of this CTA's elements, loaded once
     const Tile<L, true, W0> tl(a.geo, cta, t); // batch index = operand * W + product
-    const long long op = tl.b[0] / a.W, p = tl.b[0] - op * a.W;
+    const long long op = tl.b(0) / a.W, p = tl.b(0) - op * a.W;
     const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M;
     int vlo[RPT], vhi[RPT];
 #pragma unroll
     for (int r = 0; r < RPT; r++)
     {
-        vlo[r] = __ldcs(src + tl.j[r]);
-        vhi[r] = __ldcs(src + tl.j[r] + M);
+        vlo[r] = __ldcs(src + tl.j(r));
+        vhi[r] = __ldcs(src + tl.j(r) + M);
     }
     TwCtx c;
     c.g = tl.g;
@@ -160,13 +160,13 @@ template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const Spl
         {
             const cx<float> f = mk<float>((float)split_digit((long long)vlo[r] + a.voff, l, a.w, a.k),
                                           (float)split_digit((long long)vhi[r] + a.voff, l, a.w, a.k));
-            x[0][r] = cmul<float>(f, ldg<float>(a.twist + tl.j[r]));
+            x[0][r] = cmul<float>(f, ldg<float>(a.twist + tl.j(r)));
         }
         if (l > 0) __syncthreads();
         run_rounds<float, true, QOFF, L, 1>(x, sm, a.roots, c, t);
         cx<float>* dst = a.spec + ((op * a.k + l) * a.W + p) * M;
 #pragma unroll
-        for (int r = 0; r < RPT; r++) dst[to.j[r]] = x[0][r];
+        for (int r = 0; r < RPT; r++) dst[to.j(r)] = x[0][r];
     }
 }
 
@@ -203,28 +203,28 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            if (ti.b[r] >= a.batch)
+            if (ti.b(r) >= a.batch)
             {
                 x[0][r] = mk<float>(0.f, 0.f);
                 continue;
             }
             if (SINGLE)
             {
-                const int32_t* src = (op == 0 ? a.a : a.b) + ti.b[r] * 2 * M + ti.j[r];
+                const int32_t* src = (op == 0 ? a.a : a.b) + ti.b(r) * 2 * M + ti.j(r);
                 const long long v0 = (long long)__ldg(src) + a.voff, v1 = (long long)__ldg(src + M) + a.voff;
                 const cx<float> f = mk<float>((float)split_digit(v0, l, a.w, K), (float)split_digit(v1, l, a.w, K));
-                x[0][r] = cmul<float>(f, ldg<float>(a.twist + ti.j[r]));
+                x[0][r] = cmul<float>(f, ldg<float>(a.twist + ti.j(r)));
             }
             else
             {
-                x[0][r] = a.spec[((long long)tau * a.W + ti.b[r]) * M + ti.j[r]];
+                x[0][r] = a.spec[((long long)tau * a.W + ti.b(r)) * M + ti.j(r)];
             }
         }
         if (tau > 0) __syncthreads();
         run_rounds<float, true, 0, L, 1>(x, sm, a.roots, c, t);
 #pragma unroll
         for (int r = 0; r < RPT; r++)
-            if (tm.b[r] < a.batch) a.spec[((long long)tau * a.W + tm.b[r]) * M + tm.j[r]] = x[0][r];
+            if (tm.b(r) < a.batch) a.spec[((long long)tau * a.W + tm.b(r)) * M + tm.j(r)] = x[0][r];
     }
 
     // 2. group sums C^_s = sum_{i+j=s} A^_i B^_j (+ the centring term), four
@@ -239,11 +239,11 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
         for (int q = 0; q < 4; q++)
         {
             const int r = 4 * ch + q;
-            const bool ok = tm.b[r] < a.batch;
+            const bool ok = tm.b(r) < a.batch;
 #pragma unroll
             for (int tau = 0; tau < 2 * K; tau++)
-                v[tau][q] = ok ? a.spec[((long long)tau * a.W + tm.b[r]) * M + tm.j[r]] : mk<float>(0.f, 0.f);
-            u[q] = (a.K && ok) ? ldg<float>(a.uspec + tm.j[r]) : mk<float>(0.f, 0.f);
+                v[tau][q] = ok ? a.spec[((long long)tau * a.W + tm.b(r)) * M + tm.j(r)] : mk<float>(0.f, 0.f);
+            u[q] = (a.K && ok) ? ldg<float>(a.uspec + tm.j(r)) : mk<float>(0.f, 0.f);
         }
 #pragma unroll
         for (int sg = 0; sg < NG; sg++)
@@ -268,7 +268,7 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
                             acc = cadd<float>(acc, cmul<float>(mk<float>(e.x * uscale, e.y * uscale), u[q]));
                         }
                 }
-                if (tm.b[r] < a.batch) a.group[((long long)sg * a.W + tm.b[r]) * M + tm.j[r]] = acc;
+                if (tm.b(r) < a.batch) a.group[((long long)sg * a.W + tm.b(r)) * M + tm.j(r)] = acc;
             }
         }
     }
@@ -285,7 +285,7 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
         cx<float> x[1][RPT];
         cx<float>* grp = a.group + (long long)sg * a.W * M;
 #pragma unroll
-        for (int r = 0; r < RPT; r++) x[0][r] = (tm.b[r] < a.batch) ? grp[tm.b[r] * M + tm.j[r]] : mk<float>(0.f, 0.f);
+        for (int r = 0; r < RPT; r++) x[0][r] = (tm.b(r) < a.batch) ? grp[tm.b(r) * M + tm.j(r)] : mk<float>(0.f, 0.f);
         __syncthreads();
         run_rounds<float, false, 0, L, 1>(x, sm, a.inv_roots, c, t);
         if (SINGLE)
@@ -294,9 +294,9 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
 #pragma unroll
             for (int r = 0; r < RPT; r++)
             {
-                if (te.b[r] >= a.batch) continue;
+                if (te.b(r) >= a.batch) continue;
                 const cx<float> v =
-                    cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j[r]));
+                    cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j(r)));
                 const float rr = rintf(v.x), ri = rintf(v.y);
                 err = fmaxf(err, group_error(v, rr, ri));
                 acc_lo[r] += (long long)((unsigned long long)(long long)rr << sh);
@@ -310,7 +310,7 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
             __syncthreads();
 #pragma unroll
             for (int r = 0; r < RPT; r++)
-                if (te.b[r] < a.batch) grp[te.b[r] * M + te.j[r]] = x[0][r];
+                if (te.b(r) < a.batch) grp[te.b(r) * M + te.j(r)] = x[0][r];
         }
     }
     if (SINGLE)
@@ -318,10 +318,10 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
 #pragma unroll
         for (int r = 0; r < RPT; r++)
         {
-            if (te.b[r] >= a.batch) continue;
-            int64_t* dst = a.c + te.b[r] * 2 * M + te.j[r];
-            __stcs(reinterpret_cast<long long*>(dst), acc_lo[r] + uu_term(a, te.j[r], 2 * M));
-            __stcs(reinterpret_cast<long long*>(dst + M), acc_hi[r] + uu_term(a, te.j[r] + M, 2 * M));
+            if (te.b(r) >= a.batch) continue;
+            int64_t* dst = a.c + te.b(r) * 2 * M + te.j(r);
+            __stcs(reinterpret_cast<long long*>(dst), acc_lo[r] + uu_term(a, te.j(r), 2 * M));
+            __stcs(reinterpret_cast<long long*>(dst + M), acc_hi[r] + uu_term(a, te.j(r) + M, 2 * M));
         }
         report_err(a.max_err, err);
     }
@@ -348,7 +348,7 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
     c.s0 = 0;
     c.neg = 0;
     c.vec = tw_vec_ok<float>(a.roots) && tw_vec_ok<float>(a.inv_roots);
-    const long long p = ti.b[0];
+    const long long p = ti.b(0);
 
     long long acc_lo[RPT], acc_hi[RPT];
 #pragma unroll
@@ -359,7 +359,7 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
         const cx<float>* src = a.group + ((long long)s * a.W + p) * M;
         cx<float> x[1][RPT];
 #pragma unroll
-        for (int r = 0; r < RPT; r++) x[0][r] = src[ti.j[r]];
+        for (int r = 0; r < RPT; r++) x[0][r] = src[ti.j(r)];
         if (s > 0) __syncthreads();
         run_rounds<float, false, QOFF, L, 1>(x, sm, a.inv_roots, c, t);
         const int sh = a.w * s;
@@ -367,7 +367,7 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
         for (int r = 0; r < RPT; r++)
         {
             const cx<float> v =
-                cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j[r]));
+                cmul<float>(cmul<float>(x[0][r], mk<float>(a.scale, 0.f)), ldg<float>(a.untwist + te.j(r)));
             const float rr = rintf(v.x), ri = rintf(v.y);
             err = fmaxf(err, group_error(v, rr, ri));
             acc_lo[r] += (long long)((unsigned long long)(long long)rr << sh);
@@ -378,8 +378,8 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
 #pragma unroll
     for (int r = 0; r < RPT; r++)
     {
-        __stcs(reinterpret_cast<long long*>(dst + te.j[r]), acc_lo[r] + uu_term(a, te.j[r], 2 * M));
-        __stcs(reinterpret_cast<long long*>(dst + te.j[r] + M), acc_hi[r] + uu_term(a, te.j[r] + M, 2 * M));
+        __stcs(reinterpret_cast<long long*>(dst + te.j(r)), acc_lo[r] + uu_term(a, te.j(r), 2 * M));
+        __stcs(reinterpret_cast<long long*>(dst + te.j(r) + M), acc_hi[r] + uu_term(a, te.j(r) + M, 2 * M));
     }
     report_err(a.max_err, err);
 }
