@@ -57,6 +57,8 @@ template <typename T> struct PassArgs
     int in_kind, out_kind;
     int zero_pad; // forward first pass: the upper half of each input is zero
     int do_scale; // last inverse pass: multiply by scale
+    int perm;     // contiguous 12-stage pass: forward stores, inverse loads, each
+                  // 4096-point tile in the order e -> (e >> 4) + 256 (e & 15)
 };
 
 // Where the 16 registers of thread t (window W) live, for a CTA `cta` of a
@@ -299,9 +301,15 @@ __device__ __forceinline__ RealRows<T> real_rows(const PassArgs<T>& a, int kind,
 }
 
 // One pass of CTA-tile `cta` (sm: SMEM_ELEMS complex elements of shared memory).
-template <typename T, bool FWD, int L, bool STRIDED>
+// PERM (contiguous 12-stage passes whose spectra are only consumed pointwise
+// and by the matching inverse pass): a forward pass stores the registers of its
+// last round (window 0: thread t holds tile points 16 t + r) at the window-8
+// addresses t + 256 r, and an inverse pass loads that order straight into
+// window 0 -- one shared-memory transpose fewer each.
+template <typename T, bool FWD, int L, bool STRIDED, bool PERM = false>
 __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, cx<T>* sm)
 {
+    static_assert(!PERM || (L == EBITS && !STRIDED), "PERM: contiguous 12-stage passes only");
     constexpr int QOFF = STRIDED ? EBITS - L : 0;
     using S = Sched<QOFF, L>;
     constexpr int W0 = S::win(0, FWD), WL = S::win(S::n - 1, FWD);
@@ -360,9 +368,9 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
     c.s0 = a.geo.s0;
     c.neg = a.geo.neg;
     c.vec = tw_vec_ok<T>(a.table);
-    if constexpr (WIN != W0) transpose<T, WIN, W0, 1>(x, sm, t);
+    if constexpr (WIN != W0 && !PERM) transpose<T, WIN, W0, 1>(x, sm, t);
     run_rounds<T, FWD, QOFF, L, 1>(x, sm, a.table, c, t);
-    if constexpr (WOUT != WL) transpose<T, WL, WOUT, 1>(x, sm, t);
+    if constexpr (WOUT != WL && !PERM) transpose<T, WL, WOUT, 1>(x, sm, t);
     {
         const Tile<L, STRIDED, WOUT> tl(a.geo, cta, t);
         const int kind = a.out_kind;
@@ -403,11 +411,11 @@ __device__ __forceinline__ void pass_body(const PassArgs<T>& a, long long cta, c
 // data registers per thread and fit three CTAs; double passes fit two.
 template <typename T> constexpr int pass_min_blocks() { return sizeof(T) == 4 ? 3 : 2; }
 
-template <typename T, bool FWD, int L, bool STRIDED>
+template <typename T, bool FWD, int L, bool STRIDED, bool PERM = false>
 __global__ void __launch_bounds__(NTHR, pass_min_blocks<T>()) pass_kernel(const PassArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    pass_body<T, FWD, L, STRIDED>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
+    pass_body<T, FWD, L, STRIDED, PERM>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
 }
 
 // Algorithmic bytes of one pass launch: every element of the pass read once in
@@ -625,16 +633,20 @@ static inline PassGeo pass_geo(const Plan& p, int k, int m, int neg, long long b
     return G;
 }
 
-template <typename T, bool FWD, int L, bool STRIDED>
+template <typename T, bool FWD, int L, bool STRIDED, bool PERM = false>
 static inline int launch_pass_shape(const PassArgs<T>& a, long long ctas, cudaStream_t s)
 {
+    if constexpr (L == EBITS && !STRIDED && !PERM)
+    {
+        if (a.perm) return launch_pass_shape<T, FWD, L, false, true>(a, ctas, s);
+    }
     const size_t smem = sizeof(cx<T>) * SMEM_ELEMS;
     static int smem_done[64] = {0};
-    int st = ensure_smem(pass_kernel<T, FWD, L, STRIDED>, smem, smem_done);
+    int st = ensure_smem(pass_kernel<T, FWD, L, STRIDED, PERM>, smem, smem_done);
     if (st) return st;
     GF_TRACE(tr, pass_alg_bytes(a), s, "pass_kernel<%s,%s,L%d,%s>", sizeof(T) == 4 ? "f32" : "f64",
              kind_name(FWD), L, STRIDED ? "strided" : "contiguous");
-    pass_kernel<T, FWD, L, STRIDED><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
+    pass_kernel<T, FWD, L, STRIDED, PERM><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
     return check_launch();
 }
 
@@ -649,7 +661,8 @@ static inline int launch_pass(const PassArgs<T>& a, const Plan& p, int k, long l
     {
         // a contiguous 12-stage pass over few tiles: spread each tile over a cluster
         const bool ck = FWD ? a.in_kind == IN_CPX : (a.in_kind == IN_CPX || a.in_kind == IN_PROD);
-        if (L == EBITS && a.geo.m > EBITS && ck && a.out_kind == OUT_CPX && !a.zero_pad && cluster_ok(ctas))
+        if (L == EBITS && a.geo.m > EBITS && ck && a.out_kind == OUT_CPX && !a.zero_pad && !a.perm &&
+            cluster_ok(ctas))
         {
             ClusterArgs<T> c{};
             c.in = static_cast<const cx<T>*>(a.in);

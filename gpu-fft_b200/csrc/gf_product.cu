@@ -33,7 +33,9 @@ namespace gfb
 // in the transform's output order: at frequency k = bitrev_m(r),
 //     U = sum_j (1+i) psi^j w^(jk) = 2 / (1 - e^{i theta}) = 1 + i cot(theta/2),
 // theta = pi (4k+1) / (2M). The split-precision product uses it to centre its
-// inputs without an integer prefix scan.
+// inputs without an integer prefix scan; for M > 4096 it is stored in that
+// product's spectrum order (each 4096-point tile permuted e -> (e >> 4) +
+// 256 (e & 15)).
 // ---------------------------------------------------------------------------
 template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
 {
@@ -57,7 +59,10 @@ template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
         const unsigned k = (m > 0) ? (__brev((unsigned)i) >> (32 - m)) : 0u;
         double sh, ch;
         sincospi((4.0 * (double)k + 1.0) / (4.0 * (double)M), &sh, &ch);
-        tab[2 * H + 2 * M + i] = mk<T>((T)1, (T)(ch / sh));
+        // M > 4096: in the split product's spectrum order, each 4096-point tile
+        // permuted e -> (e >> 4) + 256 (e & 15)
+        const long long pu = (m > EBITS) ? ((i & ~4095LL) | ((i & 4095) >> 4) | ((i & 15) << 8)) : i;
+        tab[2 * H + 2 * M + pu] = mk<T>((T)1, (T)(ch / sh));
     }
 }
 

@@ -236,6 +236,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
             q.batch = 2 * k * wv;
             q.in_kind = IN_CPX;
             q.out_kind = OUT_CPX;
+            q.perm = m > EBITS; // the spectra are only read pointwise and by the inverse pass
             st = launch_pass<T, true>(q, p, kc, ctas, s);
             if (st) return st;
         }
@@ -261,6 +262,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
             q.batch = (2 * k - 1) * wv;
             q.in_kind = IN_CPX;
             q.out_kind = OUT_CPX;
+            q.perm = m > EBITS;
             st = launch_pass<T, false>(q, p, kc, ctas, s);
             if (st) return st;
         }

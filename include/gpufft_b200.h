@@ -150,8 +150,10 @@ int gpufft_host_ffnt_tables_f64(int n, void* roots, void* inv_roots, void* twist
  * range, n_power in [2, 25]). The first four hold the values of
  * FFNT<T>::ReverseRootTable_ffnt, InverseReverseRootTable_ffnt,
  * twist_table_ffnt, untwist_table_ffnt (reference fft_cpu.cu:435-473); U is
- * the transform of the all-ones polynomial (used by the split product). All
- * are computed on the device with sincospi. */
+ * the transform of the all-ones polynomial (used by the split product; for
+ * N > 8192 stored in that product's spectrum order, each block of 4096
+ * entries permuted e -> (e >> 4) + 256 (e & 15)). All are computed on the
+ * device with sincospi. */
 size_t gpufft_ffnt_tables_count(int n_power);
 int gpufft_ffnt_make_tables_f32(int n_power, void* tables, gpufft_stream_t stream);
 int gpufft_ffnt_make_tables_f64(int n_power, void* tables, gpufft_stream_t stream);
