@@ -464,8 +464,12 @@ __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitA
     }
 }
 
+// FP32 columns of 8 points fit 128 registers: four CTAs (16 warps) per
+// SM keep more group loads in flight.
+template <typename T, int L0> constexpr int inv0_col_min_blocks() { return (sizeof(T) == 4 && L0 == 3) ? 4 : 1; }
+
 template <typename T, int L0, int K>
-__global__ void __launch_bounds__(SPLIT_COL_THREADS) split_inv0_col(const SplitArgsT<T> a)
+__global__ void __launch_bounds__(SPLIT_COL_THREADS, inv0_col_min_blocks<T, L0>()) split_inv0_col(const SplitArgsT<T> a)
 {
     constexpr int R = 1 << L0;
     const int m = a.geo.m;
