@@ -96,12 +96,14 @@ def lib() -> ctypes.CDLL:
         L.gpufft_linear_mul_vjp_workspace_bytes.argtypes = [i, i]
         L.gpufft_linear_mul_vjp_workspace_bytes.restype = sz
         L.gpufft_linear_mul_vjp_f32.argtypes = [vp, vp, vp, vp, vp, i, i, vp, vp, sz, vp]
+        L.gpufft_conv_vjp_f32.argtypes = [vp, vp, vp, vp, vp, i, i, vp, vp, sz, vp]
         ll = ctypes.c_longlong
         vpp = ctypes.POINTER(ctypes.c_void_p)
         L.gpufft_batch_plan_create.argtypes = [vpp, ctypes.POINTER(ctypes.c_int), i, i, vp]
         L.gpufft_batch_plan_layout.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ll),
                                                ctypes.POINTER(ll)]
         L.gpufft_batch_plan_execute.argtypes = [vp, vp, vp, vp, vp]
+        L.gpufft_batch_plan_run.argtypes = [vp, vp, vp, vp, vp]
         L.gpufft_batch_plan_autotune.argtypes = [vp, vp, vp, vp, ctypes.c_char_p, vp]
         L.gpufft_batch_plan_capture.argtypes = [vp, vp, vp, vp, vp]
         L.gpufft_batch_plan_replay.argtypes = [vp, vp]

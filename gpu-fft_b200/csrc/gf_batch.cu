@@ -601,6 +601,12 @@ extern "C" int gpufft_batch_plan_execute(gpufft_batch_plan plan, const void* a, 
     return gfb::batch_execute(reinterpret_cast<gfb::BatchPlan*>(plan), a, b, c, (cudaStream_t)stream);
 }
 
+extern "C" int gpufft_batch_plan_run(gpufft_batch_plan plan, const void* a, const void* b, void* c,
+                                     gpufft_stream_t stream)
+{
+    return gpufft_batch_plan_execute(plan, a, b, c, stream);
+}
+
 extern "C" int gpufft_batch_plan_autotune(gpufft_batch_plan plan, const void* a, const void* b, void* c,
                                           const char* cache_path, gpufft_stream_t stream)
 {

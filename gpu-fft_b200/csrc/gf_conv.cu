@@ -232,3 +232,11 @@ extern "C" int gpufft_linear_mul_vjp_f32(const float* g, const float* a, const f
     return gfb::linear_vjp(g, a, b, grad_a, grad_b, n_power, batch, tables, workspace, workspace_bytes,
                            (cudaStream_t)stream);
 }
+
+extern "C" int gpufft_conv_vjp_f32(const float* g, const float* a, const float* b, float* grad_a, float* grad_b,
+                                   int n_power, int batch, const void* tables, void* workspace, size_t workspace_bytes,
+                                   gpufft_stream_t stream)
+{
+    return gpufft_linear_mul_vjp_f32(g, a, b, grad_a, grad_b, n_power, batch, tables, workspace, workspace_bytes,
+                                     stream);
+}

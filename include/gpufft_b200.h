@@ -235,6 +235,10 @@ size_t gpufft_linear_mul_vjp_workspace_bytes(int n_power, int batch);
 int gpufft_linear_mul_vjp_f32(const float* g, const float* a, const float* b, float* grad_a, float* grad_b,
                               int n_power, int batch, const void* tables, void* workspace, size_t workspace_bytes,
                               gpufft_stream_t stream);
+/* The same entry point under the name the path's survey proposed for it. */
+int gpufft_conv_vjp_f32(const float* g, const float* a, const float* b, float* grad_a, float* grad_b, int n_power,
+                        int batch, const void* tables, void* workspace, size_t workspace_bytes,
+                        gpufft_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* Batched products of mixed ring sizes (no reference counterpart: the      */
@@ -256,6 +260,8 @@ int gpufft_batch_plan_layout(gpufft_batch_plan plan, int* order, long long* offs
 /* c = a * b for every request on `stream`: one persistent launch, or (when
  * the autotuner found it faster) one fused chain per ring-size class. */
 int gpufft_batch_plan_execute(gpufft_batch_plan plan, const void* a, const void* b, void* c, gpufft_stream_t stream);
+/* Alias of gpufft_batch_plan_execute (create / run / destroy naming). */
+int gpufft_batch_plan_run(gpufft_batch_plan plan, const void* a, const void* b, void* c, gpufft_stream_t stream);
 /* Time the candidates on these buffers and keep the fastest: the persistent
  * launch with 1 or 2 CTAs per SM and 1, 2 or 4 work items per grab, and the
  * per-class fused chains (reported as 0 CTAs per SM by _info). cache_path (may

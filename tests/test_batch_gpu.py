@@ -49,6 +49,11 @@ def test_batch_matches_per_size_launches(gf, O, dev, dtype):
         for i in range(len(n_powers)):
             assert torch.equal(got[i], ref[i]), (shape, i, n_powers[i])
     assert plan.status() == 0
+    # gpufft_batch_plan_run is the same entry point
+    c_run = torch.empty_like(a)
+    gf.check(gf.lib().gpufft_batch_plan_run(plan.h, a.data_ptr(), b.data_ptr(), c_run.data_ptr(), None), "run")
+    torch.cuda.synchronize()
+    assert torch.equal(c_run, c)
     if dtype == torch.float64:  # |c| < 2^47: exact
         for i in rng.choice(len(n_powers), 6, replace=False):
             n = 1 << n_powers[i]

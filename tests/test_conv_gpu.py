@@ -61,10 +61,21 @@ def test_vjp_vs_direct_correlation(gf, dev, n_power, batch):
     a = rng.standard_normal((batch, n)).astype(np.float32)
     b = rng.standard_normal((batch, n)).astype(np.float32)
     g = rng.standard_normal((batch, 2 * n)).astype(np.float32)
-    ga, gb = gf.linear_mul_vjp(*(torch.from_numpy(x).to(dev) for x in (g, a, b)))
+    gd, ad, bd = (torch.from_numpy(x).to(dev) for x in (g, a, b))
+    ga, gb = gf.linear_mul_vjp(gd, ad, bd)
     wa, wb = np_vjp(g.astype(np.float64), a.astype(np.float64), b.astype(np.float64))
     assert rel(ga.cpu().numpy(), wa) < 2e-5
     assert rel(gb.cpu().numpy(), wb) < 2e-5
+    # gpufft_conv_vjp_f32 is the same entry point
+    L = gf.lib()
+    tables = gf.ffnt_tables(n_power + 1, "f32", dev)
+    ws = torch.empty(max(1, int(L.gpufft_linear_mul_vjp_workspace_bytes(n_power, batch))), dtype=torch.uint8,
+                     device=dev)
+    ga2, gb2 = torch.empty_like(ad), torch.empty_like(bd)
+    gf.check(L.gpufft_conv_vjp_f32(gd.data_ptr(), ad.data_ptr(), bd.data_ptr(), ga2.data_ptr(), gb2.data_ptr(),
+                                   n_power, batch, tables.data_ptr(), ws.data_ptr(), ws.numel(), None), "conv_vjp")
+    torch.cuda.synchronize()
+    assert torch.equal(ga2, ga) and torch.equal(gb2, gb)
 
 
 def test_vjp_n16384_batch512_finite_differences(gf, dev):
