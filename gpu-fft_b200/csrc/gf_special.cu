@@ -16,7 +16,13 @@
 // coalesced as they stand; the pass of spans 1..8 (p0 = 0), whose columns are
 // 16 consecutive points, stages 2048-point runs through padded shared memory
 // so that its global loads and stores stay coalesced too.
-#include "gf_engine.cuh"
+//
+// Launches with few 4096-point tiles (small batches, vectors of >= 4096
+// points) instead run the twelve smallest spans of every aligned tile as one
+// pass on an 8-CTA thread-block cluster (the layouts and DSMEM exchange of
+// gf_cluster.cuh): span 2^q of the tile is e-bit q, and its twiddle depends on
+// the bits below q, table[2^q + (e mod 2^q)].
+#include "gf_cluster.cuh"
 
 namespace gfb
 {
@@ -145,6 +151,116 @@ __global__ void __launch_bounds__(SPECIAL_THREADS) special_first_kernel(const Sp
     }
 }
 
+// Radix-8 round of the special network on the e-bits [P, P+3) held by register
+// bits [0, 3): the forward runs them upwards with Cooley-Tukey butterflies, the
+// inverse downwards with Gentleman-Sande. ebase is the thread's e with those
+// bits clear; the lower point of a pair at e-bit q = P + i uses
+// table[2^q + (ebase mod 2^P) + ((r mod 2^i) << P)].
+template <typename T, bool FWD, int P>
+__device__ __forceinline__ void special_cl_round(cx<T> (&x)[1][8], int ebase, const cx<T>* __restrict__ tab)
+{
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+    {
+        const int i = FWD ? k : 2 - k;
+        const cx<T>* tw = tab + (1 << (P + i)) + (ebase & ((1 << P) - 1));
+        cx<T> w[4];
+#pragma unroll
+        for (int h = 0; h < (1 << i); h++) w[h] = ldg<T>(tw + (h << P));
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+        {
+            if (r & (1 << i)) continue;
+            const cx<T> wt = w[r & ((1 << i) - 1)];
+            if (FWD)
+                ct_bfly<T>(x[0][r], x[0][r | (1 << i)], wt);
+            else
+                gs_bfly<T>(x[0][r], x[0][r | (1 << i)], wt);
+        }
+    }
+}
+
+// Spans 2^0 .. 2^11 of every 4096-point tile (vectors of 2^m >= 4096 points),
+// one tile per cluster. Forward: Y3, Y2, Y1 rounds, exchange, X round;
+// inverse: the reverse, scaled by mod_inverse when it ends the transform.
+template <typename T, bool FWD>
+__global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) special_cluster_kernel(const SpecialArgs<T> a)
+{
+    __shared__ __align__(16) cx<T> ybuf[1][CL_SMEM];
+    __shared__ __align__(16) cx<T> xbuf[1][CL_SMEM];
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int c = (int)cluster.block_rank();
+    const int t = threadIdx.x;
+    const long long row = (long long)(blockIdx.x / CL_CTAS) << EBITS; // tiles are aligned inside vectors
+    const int ex = 64 * c + t; // X layout: e = ex + 512 k
+    const int ey = 512 * c;    // Y layouts: e = ey + l
+    cx<T> x[1][8];
+    if constexpr (FWD)
+    {
+#pragma unroll
+        for (int r = 0; r < 8; r++) x[0][r] = a.data[row + ey + ypos<1>(t, r)];
+        // every CTA of the cluster runs before any writes into its shared memory
+        cluster.sync();
+        cl_transpose<T, 1, 3, 1>(x, ybuf, t);
+        special_cl_round<T, true, 0>(x, ey + ypos<3>(t, 0), a.table);
+        cl_transpose<T, 3, 2, 1>(x, ybuf, t);
+        special_cl_round<T, true, 3>(x, ey + ypos<2>(t, 0), a.table);
+        cl_transpose<T, 2, 1, 1>(x, ybuf, t);
+        special_cl_round<T, true, 6>(x, ey + ypos<1>(t, 0), a.table);
+        // Y1 -> X: point e = 512 c + t + 64 r belongs to CTA r, thread t, register c
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+        {
+            cx<T>* dst = cluster.map_shared_rank(&xbuf[0][0], r);
+            dst[cpad(64 * c + t)] = x[0][r];
+        }
+        cluster.sync();
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[0][k] = xbuf[0][cpad(64 * k + t)];
+        special_cl_round<T, true, 9>(x, ex, a.table);
+#pragma unroll
+        for (int k = 0; k < 8; k++) a.data[row + ex + 512 * k] = x[0][k];
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[0][k] = a.data[row + ex + 512 * k];
+        cluster.sync();
+        special_cl_round<T, false, 9>(x, ex, a.table);
+        // X -> Y1: register k to CTA k at local point ex
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+        {
+            cx<T>* dst = cluster.map_shared_rank(&ybuf[0][0], k);
+            dst[cpad(ex)] = x[0][k];
+        }
+        cluster.sync();
+#pragma unroll
+        for (int r = 0; r < 8; r++) x[0][r] = ybuf[0][cpad(ypos<1>(t, r))];
+        special_cl_round<T, false, 6>(x, ey + ypos<1>(t, 0), a.table);
+        cl_transpose<T, 1, 2, 1>(x, ybuf, t);
+        special_cl_round<T, false, 3>(x, ey + ypos<2>(t, 0), a.table);
+        cl_transpose<T, 2, 3, 1>(x, ybuf, t);
+        special_cl_round<T, false, 0>(x, ey + ypos<3>(t, 0), a.table);
+        cl_transpose<T, 3, 1, 1>(x, ybuf, t);
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+        {
+            const cx<T> v = a.do_scale ? cmul<T>(x[0][r], a.scale) : x[0][r];
+            a.data[row + ey + ypos<1>(t, r)] = v;
+        }
+    }
+}
+
+template <typename T, bool FWD> static int launch_special_cluster(const SpecialArgs<T>& a, cudaStream_t s)
+{
+    const long long tiles = (a.batch << a.m) >> EBITS;
+    GF_TRACE(tr, (double)(a.batch << a.m) * 2 * sizeof(cx<T>), s, "special_cluster<%s,%s>",
+             sizeof(T) == 4 ? "f32" : "f64", FWD ? "fwd" : "inv");
+    special_cluster_kernel<T, FWD><<<(unsigned)(tiles * CL_CTAS), CL_THREADS, 0, s>>>(a);
+    return check_launch();
+}
+
 template <typename T, bool FWD> static int launch_special_pass(const SpecialArgs<T>& a, int L, cudaStream_t s)
 {
     const long long points = a.batch << a.m;
@@ -174,11 +290,14 @@ static int special_fft(cx<T>* inout, const cx<T>* table, int n_power, int fft_ty
     if (!inout || !table || batch <= 0 || (fft_type != GPUFFT_FORWARD && fft_type != GPUFFT_INVERSE))
         return GPUFFT_ERROR_INVALID_VALUE;
     if ((uintptr_t)inout % sizeof(cx<T>) || (uintptr_t)table % sizeof(cx<T>)) return GPUFFT_ERROR_MISALIGNED;
+    // few tiles: the twelve smallest spans as one cluster pass (L = 12 below)
+    const long long tiles = ((long long)batch << n_power) >> EBITS;
+    const bool cl = n_power >= EBITS && cluster_ok(tiles);
     int p0s[8], Ls[8], np = 0;
-    for (int p0 = 0; p0 < n_power; p0 += 4)
+    for (int p0 = 0; p0 < n_power; p0 += (cl && p0 == 0) ? EBITS : 4)
     {
         p0s[np] = p0;
-        Ls[np] = (n_power - p0) < 4 ? (n_power - p0) : 4;
+        Ls[np] = (cl && p0 == 0) ? EBITS : ((n_power - p0) < 4 ? (n_power - p0) : 4);
         np++;
     }
     SpecialArgs<T> a{};
@@ -192,8 +311,13 @@ static int special_fft(cx<T>* inout, const cx<T>* table, int n_power, int fft_ty
         const int k = fft_type == GPUFFT_FORWARD ? i : np - 1 - i;
         a.p0 = p0s[k];
         a.do_scale = fft_type == GPUFFT_INVERSE && i == np - 1;
-        const int st = fft_type == GPUFFT_FORWARD ? launch_special_pass<T, true>(a, Ls[k], s)
-                                                  : launch_special_pass<T, false>(a, Ls[k], s);
+        int st;
+        if (Ls[k] == EBITS)
+            st = fft_type == GPUFFT_FORWARD ? launch_special_cluster<T, true>(a, s)
+                                            : launch_special_cluster<T, false>(a, s);
+        else
+            st = fft_type == GPUFFT_FORWARD ? launch_special_pass<T, true>(a, Ls[k], s)
+                                            : launch_special_pass<T, false>(a, Ls[k], s);
         if (st) return st;
     }
     return GPUFFT_SUCCESS;

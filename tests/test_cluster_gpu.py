@@ -116,3 +116,28 @@ def test_ffnt_dropin_cluster_identical(gf, O, dev, both, n_power):
 
     on, off = both(run)
     assert torch.equal(on, off)
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+@pytest.mark.parametrize("n_power,batch", [(12, 1), (13, 3), (16, 1), (18, 2)])
+def test_special_fft_cluster_identical(gf, dev, both, T, n_power, batch):
+    # GPU_Special_FFT forward then inverse on random vectors and a random table of
+    # 2^n_power entries: the twelve smallest spans run on clusters or as column passes
+    rng = np.random.default_rng(400 + n_power)
+    M = 1 << n_power
+    C = np.complex128 if T == np.float64 else np.complex64
+    x = (rng.standard_normal((batch, M)) + 1j * rng.standard_normal((batch, M))).astype(C)
+    tab = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(C)
+    d_tab = torch.from_numpy(tab).to(dev)
+    L = gf.lib()
+    f = L.gpufft_special_fft_f64 if T == np.float64 else L.gpufft_special_fft_f32
+
+    def run():
+        buf = torch.from_numpy(x.ravel().copy()).to(dev)
+        gf.check(f(buf.data_ptr(), d_tab.data_ptr(), n_power, 0, 1.0, 0.0, batch, None), "fwd")
+        spec = buf.clone()
+        gf.check(f(buf.data_ptr(), d_tab.data_ptr(), n_power, 1, 1.0 / M, 0.25, batch, None), "inv")
+        return torch.cat([spec, buf])
+
+    on, off = both(run)
+    assert torch.equal(on, off)
