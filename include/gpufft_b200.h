@@ -235,7 +235,7 @@ size_t gpufft_linear_mul_vjp_workspace_bytes(int n_power, int batch);
 int gpufft_linear_mul_vjp_f32(const float* g, const float* a, const float* b, float* grad_a, float* grad_b,
                               int n_power, int batch, const void* tables, void* workspace, size_t workspace_bytes,
                               gpufft_stream_t stream);
-/* The same entry point under the name the path's survey proposed for it. */
+/* Alias of gpufft_linear_mul_vjp_f32 (convolution naming). */
 int gpufft_conv_vjp_f32(const float* g, const float* a, const float* b, float* grad_a, float* grad_b, int n_power,
                         int batch, const void* tables, void* workspace, size_t workspace_bytes,
                         gpufft_stream_t stream);
