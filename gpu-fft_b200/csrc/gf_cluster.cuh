@@ -68,6 +68,14 @@ template <typename T> struct ClusterArgs
 
 __device__ __forceinline__ int cpad(int l) { return l + (l >> 3); }
 
+// The first cluster barrier only has to show that every CTA of the cluster is
+// running (its shared memory exists) before DSMEM stores reach it: a relaxed
+// arrive right after the global loads are issued, and the wait just before the
+// first remote store, so the barrier overlaps the load latency. Every thread
+// arrives and waits once.
+__device__ __forceinline__ void cl_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cl_wait() { asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory"); }
+
 // Local point of register r of thread t in layout Y1 / Y2 / Y3.
 template <int Y> __device__ __forceinline__ int ypos(int t, int r)
 {
@@ -153,8 +161,7 @@ __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) cl
             const long long i = row + ey + ypos<1>(t, r);
             x[0][r] = a.prod ? cmul<T>(a.in[i], a.in[i + a.prod_off]) : a.in[i];
         }
-        // every CTA of the cluster runs before any writes into its shared memory
-        cluster.sync();
+        cl_arrive_relaxed();
         cl_transpose<T, 1, 3, 1>(x, ybuf, t);
     }
     else
@@ -165,8 +172,9 @@ __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) cl
             x[0][k] = a.in[row + ex + 512 * k];
             if constexpr (NA == 2) x[NA - 1][k] = a.in2[row + ex + 512 * k];
         }
-        cluster.sync();
+        cl_arrive_relaxed();
         cl_round<T, true, 9, NA>(x, ex, a.table, g);
+        cl_wait(); // every CTA of the cluster runs: its shared memory can be written
         // X -> Y1: register k to CTA k at local point ex
 #pragma unroll
         for (int k = 0; k < 8; k++)
@@ -215,6 +223,7 @@ __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) cl
         cl_round<T, false, 3, 1>(z, ey + ypos<2>(t, 0), a.inv_table, g);
         cl_transpose<T, 2, 1, 1>(z, ybuf, t);
         cl_round<T, false, 6, 1>(z, ey + ypos<1>(t, 0), a.inv_table, g);
+        if constexpr (MODE == CLM_INV) cl_wait(); // the first remote store of this mode
         // Y1 -> X: point e = 512 c + t + 64 r belongs to CTA r, thread t, register c
 #pragma unroll
         for (int r = 0; r < 8; r++)

@@ -199,14 +199,14 @@ __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) sp
     {
 #pragma unroll
         for (int r = 0; r < 8; r++) x[0][r] = a.data[row + ey + ypos<1>(t, r)];
-        // every CTA of the cluster runs before any writes into its shared memory
-        cluster.sync();
+        cl_arrive_relaxed();
         cl_transpose<T, 1, 3, 1>(x, ybuf, t);
         special_cl_round<T, true, 0>(x, ey + ypos<3>(t, 0), a.table);
         cl_transpose<T, 3, 2, 1>(x, ybuf, t);
         special_cl_round<T, true, 3>(x, ey + ypos<2>(t, 0), a.table);
         cl_transpose<T, 2, 1, 1>(x, ybuf, t);
         special_cl_round<T, true, 6>(x, ey + ypos<1>(t, 0), a.table);
+        cl_wait(); // every CTA of the cluster runs: its shared memory can be written
         // Y1 -> X: point e = 512 c + t + 64 r belongs to CTA r, thread t, register c
 #pragma unroll
         for (int r = 0; r < 8; r++)
@@ -225,8 +225,9 @@ __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) sp
     {
 #pragma unroll
         for (int k = 0; k < 8; k++) x[0][k] = a.data[row + ex + 512 * k];
-        cluster.sync();
+        cl_arrive_relaxed();
         special_cl_round<T, false, 9>(x, ex, a.table);
+        cl_wait(); // every CTA of the cluster runs: its shared memory can be written
         // X -> Y1: register k to CTA k at local point ex
 #pragma unroll
         for (int k = 0; k < 8; k++)
