@@ -248,7 +248,11 @@ __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) cl
 // (0: never). Set by gpufft_set_cluster_tiles.
 extern int g_cluster_max_tiles;
 
-inline bool cluster_ok(long long tiles) { return tiles > 0 && tiles <= g_cluster_max_tiles; }
+inline bool cluster_ok(long long tiles)
+{
+    // the grid (8 CTAs per tile) must stay within the 2^31 - 1 limit of gridDim.x
+    return tiles > 0 && tiles <= g_cluster_max_tiles && tiles <= 0x7fffffffLL / CL_CTAS;
+}
 
 template <typename T, int MODE>
 static inline int launch_cluster_pass(const ClusterArgs<T>& a, long long tiles, long long rows, cudaStream_t s)
