@@ -95,3 +95,17 @@ def test_trace_collect_without_records(gf):
     # tracing is off by default; collecting with nothing recorded needs no GPU
     gf.trace_enable(False)
     assert gf.trace_collect() == []
+
+
+def test_cluster_tile_limit_roundtrip(gf):
+    # host-only setting: no device work; a negative value queries
+    prev = gf.set_cluster_tiles(-1)
+    assert prev >= 0
+    try:
+        assert gf.set_cluster_tiles(0) == prev
+        assert gf.set_cluster_tiles(-1) == 0
+        assert gf.set_cluster_tiles(1 << 30) == 0
+        assert gf.set_cluster_tiles(-5) == 1 << 30
+    finally:
+        gf.set_cluster_tiles(prev)
+    assert gf.set_cluster_tiles(-1) == prev
