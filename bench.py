@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--n-power", type=int, default=16)
     p.add_argument("--batch", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-ref-gpu", dest="ref_gpu", action="store_false",
+                   help="skip timing the reference's own GPU build beside ours (N = 1 only)")
     return p.parse_args()
 
 
@@ -170,30 +172,159 @@ def cpu_sample_count(n, threads):
     return max(threads, int(10.0 / per))
 
 
+def cpu_reference_error(n, samples=256):
+    """Largest |error| of the reference's FFNT<double>::MULT on the first product
+    of the workload (24-bit coefficients), at `samples` sampled coefficients,
+    against the exact product (int64 wrap-around semantics). The reference
+    casts its rounded doubles to unsigned long long, so the difference is taken
+    modulo 2^64 and read as signed."""
+    import numpy as np
+    import oracle as O
+    R = O.ref()
+    if R is None:
+        return None
+    a64, b64 = make_inputs(1, n, 0)
+    a = a64[0].numpy().astype(np.uint64)
+    b = b64[0].numpy().astype(np.uint64)
+    out = np.zeros(n, np.uint64)
+    R.ref_ffnt_mult_f64(n, a, b, out)
+    rng = np.random.default_rng(2)
+    idx = np.sort(rng.choice(n, samples, replace=False)).astype(np.int32)
+    want = O.wrap64(O.negacyclic_coeffs(a64[0].numpy(), b64[0].numpy(), idx))
+    diff = (out[idx].astype(np.int64) - want)  # wraps modulo 2^64
+    return float(np.max(np.abs(diff.astype(np.float64))))
+
+
+def cpu_reference_line(n, threads, reps=1):
+    """The reference's CPU product on the host cores: the bounded sample of
+    cpu_sample_count products (one per thread at a time), median of `reps`
+    repetitions; the same sample in the bench's cpu_baseline and in the
+    --impl reference arm."""
+    cnt = cpu_sample_count(n, threads)
+    vals = []
+    for _ in range(reps):
+        v, kind, cores = cpu_baseline_reference(n, cnt, threads)
+        vals.append(v)
+    err = cpu_reference_error(n)
+    return {"value": statistics.median(vals), "unit": "products/s", "cores": cores, "kind": kind,
+            "sample": f"{cnt} products of N={n} (2^{n.bit_length() - 1}), FFNT<double>::MULT, one product per "
+                      f"host thread at a time, median of {reps}",
+            "exact": False if err is None or err > 0 else True,
+            "max_abs_error_on_sample": err,
+            "note": "the reference's FP64 product is not exact at this size (results reach about 2^62, where "
+                    "an FP64 ulp is 2^10); the GPU line's split product is"}, cnt
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     n = 1 << args.n_power
     threads = os.cpu_count() or 1
-    # each step: a bounded sample of the workload's products (products/s is per-product)
-    count = max(threads, cpu_sample_count(n, threads) // 4)
+    # each step: the same bounded sample as the cpu_baseline leg of the GPU arm
+    cnt = cpu_sample_count(n, threads)
     vals = []
+    kind, cores = "reference", threads
     for i in range(args.warmup + args.steps):
-        v, kind, cores = cpu_baseline_reference(n, count, threads)
+        v, kind, cores = cpu_baseline_reference(n, cnt, threads)
         if i >= args.warmup:
             vals.append(v)
     val = statistics.median(vals)
+    err = cpu_reference_error(n)
     line = {"impl": "reference", "metric": f"negacyclic poly-mults/s at N=2^{args.n_power}", "value": val,
             "unit": "products/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": count / val * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": cnt / val * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded uniform [0, 2^24))",
             "config": {"workload": f"FFNT negacyclic product N=2^{args.n_power}, batch {args.batch}, "
                                    "coefficients in [0, 2^24)", "ring_log2": args.n_power, "batch": args.batch,
                        "l2": "inputs > L2"},
+            "exact": False if err is None or err > 0 else True, "max_abs_error_on_sample": err,
             "cpu_baseline": {"value": val, "unit": "products/s", "cores": cores, "kind": kind,
-                             "sample": f"{count} products of N=2^{args.n_power} per step, FFNT<double>::MULT"},
+                             "sample": f"{cnt} products of N=2^{args.n_power} per step, FFNT<double>::MULT, "
+                                       "one product per host thread at a time"},
             "e2e": {"value": val, "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_arm(gf, a64, b64, n_power, batch, args, dev, torch):
+    """The reference's own GPU path beside ours, on the same GPU and the same
+    FP64 inputs: its src/lib/fft.cu built for sm_100a (oracle/_ref, called
+    through its C++ API GPU_FFNT: forward of 2*batch, inverse with the product,
+    reference-format tables), this library's drop-in GPU_FFNT (the same two
+    calls) and its native FP64 and exact split products, at the workload's batch
+    and at batch 1 (the shape of the reference's own benchmark,
+    bench_gpu_ffnt_R_R_mult.cu). CUDA events around K steps after W warm-ups."""
+    import ctypes
+    import numpy as np
+    import oracle as O
+    R = O.ref_gpu()
+    if R is None:
+        return {"unavailable": "the reference's GPU build (oracle/_ref/libgpufft_ref_gpu.so) is absent"}
+    n = 1 << n_power
+    h = n // 2
+    roots, inv_roots, twist, untwist = [torch.from_numpy(np.ascontiguousarray(t)).to(dev)
+                                        for t in O.ffnt_tables(n, "f64")]
+    L = gf.lib()
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    out = {"timed": "CUDA events around K steps (each step: the two GPU_FFNT calls, or one product call)",
+           "tables": "reference-format FFNT<double> tables on the device", "cases": []}
+    for bt in (batch, 1):
+        inout = torch.cat([a64[:bt].reshape(-1), b64[:bt].reshape(-1)]).double().to(dev)
+        temp = torch.empty(bt * h, dtype=torch.complex128, device=dev)
+        chk = {}
+
+        def two(fn, ok):
+            def run():
+                st = fn(inout.data_ptr(), temp.data_ptr(), twist.data_ptr(), roots.data_ptr(), n_power, 0, 1.0,
+                        0.0, 2 * bt, 0, None)
+                st |= fn(inout.data_ptr(), temp.data_ptr(), untwist.data_ptr(), inv_roots.data_ptr(), n_power, 1,
+                         1.0 / h, 0.0, bt, 1, None)
+                ok.append(st)
+            return run
+        ok_ref, ok_ours = [], []
+        ms_ref = timed(two(R.ref_gpu_ffnt_f64, ok_ref))
+        ms_drop = timed(two(L.gpufft_ffnt_f64, ok_ours))
+        # native products on the same inputs
+        ad, bd = a64[:bt].double().to(dev), b64[:bt].double().to(dev)
+        cd = torch.empty_like(ad)
+        tf = gf.ffnt_tables(n_power, "f64", dev)
+        ws = torch.empty(max(1, gf.negacyclic_mul_workspace_bytes(n_power, bt, 64)), dtype=torch.uint8, device=dev)
+        ms_f64 = timed(lambda: gf.negacyclic_mul(ad, bd, out=cd, tables=tf, workspace=ws))
+        ai, bi = a64[:bt].to(torch.int32).to(dev), b64[:bt].to(torch.int32).to(dev)
+        ci = torch.empty((bt, n), dtype=torch.int64, device=dev)
+        w, k = gf.split_plan(n_power, 24, True)
+        t32 = gf.ffnt_tables(n_power, "f32", dev)
+        wss = torch.empty(max(1, int(L.gpufft_negacyclic_mul_split_workspace_bytes(n_power, bt, k))),
+                          dtype=torch.uint8, device=dev)
+        ms_split = timed(lambda: gf.negacyclic_mul_split(ai, bi, out=ci, input_bits=24, non_negative=True,
+                                                         limbs=(w, k), tables=t32, workspace=wss))
+        if any(ok_ref) or any(ok_ours):
+            return {"unavailable": f"a GPU_FFNT call failed (status {max(ok_ref + ok_ours)})"}
+        out["cases"].append({
+            "batch": bt, "ring_log2": n_power,
+            "ref_gpu_ms": ms_ref, "ref_gpu_value": bt / (ms_ref * 1e-3),
+            "ours_dropin_ms": ms_drop, "ours_dropin_value": bt / (ms_drop * 1e-3),
+            "ours_f64_ms": ms_f64, "ours_f64_value": bt / (ms_f64 * 1e-3),
+            "ours_split_ms": ms_split, "ours_split_value": bt / (ms_split * 1e-3),
+            "dropin_vs_ref": ms_ref / ms_drop, "f64_vs_ref": ms_ref / ms_f64, "split_vs_ref": ms_ref / ms_split})
+        del inout, temp, ad, bd, cd, ws, ai, bi, ci, wss
+        torch.cuda.empty_cache()
+    head = out["cases"][0]
+    out["ref_gpu_value"] = head["ref_gpu_value"]
+    out["unit"] = "products/s"
+    return out
 
 
 def make_path(gf, name, n_power, batch, dev, torch):
@@ -312,17 +443,17 @@ def time_path(step, host_step, a, b, c, hosts, args, stream, torch, barrier, max
     return ms, ms_e2e, t0, t1
 
 
-# DRAM traffic of the dominant kernels as a fraction of their algorithmic
-# bytes, from one ncu capture each of a smaller wave of the same kernel
-# (dram__bytes_read.sum + dram__bytes_write.sum over the kernel's algorithmic
-# bytes; ncu flushes caches before each replay, so this is the cold-cache
-# figure). Both scale with the products per launch, so traffic per launch =
-# ratio x measured algorithmic bytes per launch.
+# DRAM traffic of the dominant kernels as a fraction of the bytes the library's
+# tracing tags them with (their own inputs read once and outputs written once),
+# from one ncu capture each of a smaller wave of the same kernel
+# (dram__bytes_read.sum + dram__bytes_write.sum; ncu flushes caches before each
+# replay, so this is the cold-cache figure). Both scale with the products per
+# launch, so traffic per launch = ratio x the kernel's tagged bytes per launch.
 NCU_TRAFFIC = {
-    # wave of 46 products (3680 CTAs): 120.8 MB read + 63.5 MB written / 241.2 MB
-    "pass_kernel<f32,fwd,L12,contiguous>": (184.3 / 241.2, "profiles/pass_kernel_f32_L12_split_N65536.md"),
-    # wave of 74 products (592 CTAs): 78.2 MB read + 2.8 MB written / 116.4 MB
-    "fused_kernel<f64,L12,middle>": (81.0 / 116.4, "profiles/fused_kernel_f64_L12_N65536.md"),
+    # wave of 46 products (3680 CTAs): 120.8 MB read + 63.5 MB written of 241.2 MB tagged
+    "pass_kernel<f32,fwd,L12,contiguous>": (184.3 / 241.2, "ncu capture of a 46-product wave"),
+    # wave of 74 products (592 CTAs): 78.2 MB read + 2.8 MB written of 116.4 MB tagged
+    "fused_kernel<f64,L12,middle>": (81.0 / 116.4, "ncu capture of a 74-product wave"),
 }
 
 
@@ -342,27 +473,43 @@ def traced_kernels(gf, step, a, b, c, args, stream, torch, barrier, max_over_ran
     return rows, max_over_ranks(e0.elapsed_time(e1) / args.steps)
 
 
-def kernel_roofline(rows, peak, peak_kind, ms_traced, steps):
-    """Roofline of the dominant kernel (largest summed device time): its
-    algorithmic bytes per launch over its mean CUDA-event launch duration."""
+def kernel_roofline(rows, peak, peak_kind, ms_traced, steps, alg_per_product=None, products_per_step=None):
+    """Roofline of the dominant kernel (largest summed device time).
+
+    `achieved` / `frac` count the path's algorithmic bytes per product (the API
+    inputs read once and outputs written once: 16N for the split product, 24N
+    for the FP64 product) times the products one launch of that kernel covers,
+    over its mean CUDA-event launch duration. `kernel_bytes_gbs` /
+    `kernel_bytes_frac` count instead the bytes the kernel itself must move
+    (its own inputs and outputs, intermediate spectra included)."""
     dom = rows[0]
     per_launch_ms = dom["ms"] / dom["launches"]
     per_launch_bytes = dom["alg_bytes"] / dom["launches"]
-    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    own = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    launches_per_step = dom["launches"] / steps
     total = sum(r["ms"] for r in rows)
     traffic = NCU_TRAFFIC.get(dom["kernel"])
-    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_kind": peak_kind, "traffic": traffic[0] * per_launch_bytes if traffic else None,
-            "traffic_source": (traffic[1] + " (cold-cache ncu capture of a smaller wave, scaled by products "
-                               "per launch)") if traffic else None,
-            "kernel": dom["kernel"], "launches_per_step": dom["launches"] / steps,
-            "mean_launch_us": per_launch_ms * 1e3, "alg_bytes_per_launch": per_launch_bytes,
-            "share_of_step": dom["ms"] / total if total else None,
-            "timed": "CUDA events around each launch (library tracing) over a repeat of the timed steps",
-            "traced_ms_per_step": ms_traced,
-            "kernels": [{"kernel": r["kernel"], "launches_per_step": r["launches"] / steps,
-                         "ms_per_step": r["ms"] / steps,
-                         "gbs": (r["alg_bytes"] / (r["ms"] * 1e-3) / 1e9) if r["ms"] else None} for r in rows]}
+    out = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+           "traffic": traffic[0] * per_launch_bytes if traffic else None,
+           "traffic_source": (traffic[1] + ", scaled by products per launch") if traffic else None,
+           "kernel": dom["kernel"], "launches_per_step": launches_per_step,
+           "mean_launch_us": per_launch_ms * 1e3, "kernel_bytes_per_launch": per_launch_bytes,
+           "kernel_bytes_gbs": own, "kernel_bytes_frac": own / peak,
+           "share_of_step": dom["ms"] / total if total else None,
+           "timed": "CUDA events around each launch (library tracing) over a repeat of the timed steps",
+           "traced_ms_per_step": ms_traced,
+           "kernels": [{"kernel": r["kernel"], "launches_per_step": r["launches"] / steps,
+                        "ms_per_step": r["ms"] / steps,
+                        "gbs": (r["alg_bytes"] / (r["ms"] * 1e-3) / 1e9) if r["ms"] else None} for r in rows]}
+    if alg_per_product is not None and products_per_step:
+        per_launch_products = products_per_step / launches_per_step
+        alg = alg_per_product * per_launch_products
+        achieved = alg / (per_launch_ms * 1e-3) / 1e9
+        out.update({"achieved": achieved, "frac": achieved / peak, "alg_bytes_per_launch": alg,
+                    "alg_bytes_per_product": alg_per_product, "products_per_launch": per_launch_products})
+    else:
+        out.update({"achieved": own, "frac": own / peak, "alg_bytes_per_launch": per_launch_bytes})
+    return out
 
 
 def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, peak, peak_kind):
@@ -460,7 +607,7 @@ def run_batch(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cl
         "config": {"workload": "4096 negacyclic products, ring sizes log-uniform 2^10..2^17, FP64, one persistent "
                                "cooperative launch replayed from a CUDA graph", "requests": 4096,
                    "coefficients": plan.total, "launch_shape": info, "l2": "inputs larger than L2 (no flush)"},
-        "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps),
+        "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps, alg / 4096, 4096),
         "chain": {"achieved_gbs": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": alg,
                   "timed": "graph replay of the persistent launch, CUDA events"},
         "e2e": {"value": world * 4096 / (ms_e2e * 1e-3), "unit": "products/s", "h2d_bytes_per_step": 2 * alg // 3,
@@ -590,7 +737,7 @@ def run_vjp(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls,
         "dtype": "f32", "data": "synthetic (seeded i.i.d. N(0,1))",
         "config": {"workload": "real FP32 linear convolution N=2^14 zero-padded to 2^15, batch 512, forward + VJP",
                    "batch_per_gpu": batch, "l2": "inputs larger than L2 (no flush)"},
-        "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps),
+        "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps, alg / batch, batch),
         "chain": {"achieved_gbs": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": alg,
                   "timed": "forward product + VJP per step, CUDA events"},
         "e2e": {"value": world * batch / (ms_e2e * 1e-3), "unit": "products/s",
@@ -662,7 +809,8 @@ def run_cc(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, 
                 dropin = {"ms_per_step": ms, "products_s": world * batch / (ms * 1e-3),
                           "achieved_gbs": alg / (ms * 1e-3) / 1e9, "frac": alg / (ms * 1e-3) / 1e9 / peak,
                           "rel_l2_vs_fp64_cpu": max(errs),
-                          "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps)}
+                          "roofline": kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps, alg / batch,
+                                                      batch)}
                 # the native fused cyclic product on the same operands
                 xa = x.to(dev)
                 av, bv = xa[: batch * M].view(batch, M), xa[batch * M:].view(batch, M)
@@ -697,7 +845,8 @@ def run_cc(args, gf, dev, torch, world, rank, barrier, max_over_ranks, clk_cls, 
                 cases.append({"dtype": tag, "ring_log2": n_power, "batch": batch, "ms_per_step": nms,
                               "products_s": world * batch / (nms * 1e-3), "achieved_gbs": alg / (nms * 1e-3) / 1e9,
                               "frac": alg / (nms * 1e-3) / 1e9 / peak, "rel_l2_vs_fp64_cpu": max(nerr),
-                              "roofline": kernel_roofline(nrows, peak, peak_kind, nms_traced, args.steps),
+                              "roofline": kernel_roofline(nrows, peak, peak_kind, nms_traced, args.steps,
+                                                          alg / batch, batch),
                               "dropin_gpu_fft": dropin})
                 del x, buf, xa, av, bv, out, ws
                 torch.cuda.empty_cache()
@@ -779,7 +928,7 @@ def main():
             rows, ms_traced = traced_kernels(gf, step, a, b, c, args, stream, torch, barrier, max_over_ranks)
             achieved = alg * batch / (ms * 1e-3) / 1e9
             results[name] = dict(ms=ms, ms_e2e=ms_e2e, t0=t0, t1=t1, alg=alg, launches=launches,
-                                 kroof=kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps),
+                                 kroof=kernel_roofline(rows, peak, peak_kind, ms_traced, args.steps, alg, batch),
                                  traced_launches=sum(r["launches"] for r in rows),
                                  value=world * batch / (ms * 1e-3), achieved=achieved,
                                  h2d=2 * batch * n * a_host.element_size(), d2h=batch * n * c_host.element_size(),
@@ -833,12 +982,10 @@ def main():
             tgt = line if name == args.path else line[name]
             tgt["exact_on_sample"] = exact
             tgt["max_abs_error_on_sample"] = err
+    if rank == 0 and world == 1 and args.ref_gpu:
+        line["ref_gpu"] = reference_gpu_arm(gf, a64, b64, n_power, batch, args, dev, torch)
     if rank == 0 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        cnt = cpu_sample_count(n, threads)
-        v, kind, cores = cpu_baseline_reference(n, cnt, threads)
-        line["cpu_baseline"] = {"value": v, "unit": "products/s", "cores": cores, "kind": kind,
-                                "sample": f"{cnt} products of N=2^{n_power}, FFNT<double>::MULT, one per thread"}
+        line["cpu_baseline"], _ = cpu_reference_line(n, os.cpu_count() or 1, reps=3)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -144,6 +144,10 @@ def lib() -> ctypes.CDLL:
         L.gpufft_version.restype = i
         L.gpufft_set_cluster_tiles.argtypes = [i]
         L.gpufft_set_cluster_tiles.restype = i
+        L.gpufft_batch_plan_set_barrier.argtypes = [vp, ctypes.c_uint, ctypes.c_uint]
+        L.gpufft_set_split_tile.argtypes = [i]
+        L.gpufft_set_split_tile.restype = i
+        L.gpufft_split_wait_timeouts.argtypes = [vp, i]
         _lib = L
     return _lib
 
@@ -381,7 +385,7 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
     need = int(wsf(n_power, batch, k))
     if workspace is None:
         workspace = torch.empty(max(need, 1), dtype=torch.uint8, device=a.device)
-    err = torch.zeros(1, dtype=torch.float32, device=a.device)
+    err = torch.empty(1, dtype=torch.float32, device=a.device)  # zeroed by the call
     fn = L.gpufft_negacyclic_mul_split_f64 if f64 else L.gpufft_negacyclic_mul_split_f32
     st = fn(
         _ptr(a), _ptr(b), _ptr(out), n_power, batch, int(input_bits), int(bool(non_negative)), w, k,
@@ -394,6 +398,22 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
 # ---------------------------------------------------------------------------
 # Per-kernel device-time tracing
 # ---------------------------------------------------------------------------
+def set_split_tile(on: int) -> int:
+    """FP32 split products of rings 2^14..2^16 (up to five limbs) run their
+    contiguous stages in the shared-memory tile kernel (1, the default) or in
+    the chain of pass and group-sum kernels (0); a negative value queries.
+    The integers are the same either way. Returns the previous setting."""
+    return int(lib().gpufft_set_split_tile(int(on)))
+
+
+def split_wait_timeouts(clear: bool = True) -> int:
+    """Bounded waits of the split tile kernel that ran out since the last clear
+    (each makes its call report an infinite error). Synchronous."""
+    n = ctypes.c_uint()
+    check(lib().gpufft_split_wait_timeouts(ctypes.byref(n), int(bool(clear))), "split_wait_timeouts")
+    return n.value
+
+
 def set_cluster_tiles(max_tiles: int) -> int:
     """Contiguous 12-stage passes over at most `max_tiles` 4096-point tiles run
     as 8-CTA clusters (small batches); 0 disables, a negative value queries.
@@ -484,7 +504,7 @@ def negacyclic_mul_split_host(a, b, out=None, input_bits=24, non_negative=False,
         raise ValueError("Invalid n_power range!")
     if workspace is None:
         workspace = torch.empty(need, dtype=torch.uint8, device=dev)
-    err = torch.zeros(1, dtype=torch.float32, device=dev)
+    err = torch.empty(1, dtype=torch.float32, device=dev)  # zeroed by the call
     check(L.gpufft_negacyclic_mul_split_f32_host(
         a.data_ptr(), b.data_ptr(), out.data_ptr(), n_power, batch, int(chunk), int(input_bits),
         int(bool(non_negative)), w, k, _ptr(tables), workspace.data_ptr(),
@@ -588,6 +608,12 @@ class BatchPlan:
               "batch_plan_execute")
         return out
 
+    def set_barrier(self, max_polls=1 << 26, extra_arrivals=0):
+        """Poll limit of the persistent launch's grid barriers; extra_arrivals > 0
+        makes every barrier run out (tests of the timeout path only)."""
+        check(lib().gpufft_batch_plan_set_barrier(self.h, int(max_polls), int(extra_arrivals)),
+              "batch_plan_set_barrier")
+
     def autotune(self, a, b, out, cache_path=None, stream=None):
         cp = cache_path.encode() if cache_path else None
         check(lib().gpufft_batch_plan_autotune(self.h, _ptr(a), _ptr(b), _ptr(out), cp, _stream_handle(stream)),
@@ -672,7 +698,7 @@ class SplitBatchPlan:
         if out is None:
             out = torch.empty(self.total, dtype=torch.int64, device=a.device)
         if err is None:
-            err = torch.zeros(1, dtype=torch.float32, device=a.device)
+            err = torch.empty(1, dtype=torch.float32, device=a.device)  # zeroed by the call
         check(lib().gpufft_split_batch_plan_execute(self.h, _ptr(a), _ptr(b), _ptr(out), _ptr(err),
                                                     _stream_handle(stream)), "split_batch_plan_execute")
         return out, err

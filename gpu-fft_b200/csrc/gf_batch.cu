@@ -19,7 +19,8 @@
 // gpufft_negacyclic_mul_* calls on the same data.
 //
 // The grid barrier is a monotonic arrival counter with a bounded wait: a CTA
-// that waits longer than BARRIER_MAX_POLLS sets the plan's timeout flag and
+// that waits longer than the plan's poll limit (BARRIER_MAX_POLLS unless
+// gpufft_batch_plan_set_barrier changed it) sets the plan's timeout flag and
 // continues (the launch is cooperative, so all CTAs are co-resident and the
 // barrier normally completes in microseconds); gpufft_batch_plan_status
 // reports the flag.
@@ -79,9 +80,11 @@ template <typename T> struct BatchArgs
     unsigned nitems[3];
     unsigned* counters; // [3] work counters, [3] barrier arrivals, [1] timeout flag
     int grab;
+    unsigned max_polls;     // polls before a grid barrier gives up
+    unsigned barrier_extra; // arrivals a barrier waits for beyond the grid (0; raised only to test the timeout)
 };
 
-__device__ __forceinline__ void grid_barrier(unsigned* arrivals, unsigned target, unsigned* flag)
+__device__ __forceinline__ void grid_barrier(unsigned* arrivals, unsigned target, unsigned* flag, unsigned max_polls)
 {
     __syncthreads();
     if (threadIdx.x == 0)
@@ -91,7 +94,7 @@ __device__ __forceinline__ void grid_barrier(unsigned* arrivals, unsigned target
         unsigned polls = 0;
         while (*((volatile unsigned*)arrivals) < target)
         {
-            if (++polls > BARRIER_MAX_POLLS)
+            if (++polls > max_polls)
             {
                 atomicExch(flag, 1u);
                 break;
@@ -219,7 +222,7 @@ template <typename T, int MINB> __global__ void __launch_bounds__(NTHR, MINB) ba
                 __syncthreads(); // the next item reuses shared memory
             }
         }
-        if (ph < 2) grid_barrier(&A.counters[3 + ph], gridDim.x, &A.counters[6]);
+        if (ph < 2) grid_barrier(&A.counters[3 + ph], gridDim.x + A.barrier_extra, &A.counters[6], A.max_polls);
     }
 }
 
@@ -242,6 +245,7 @@ struct BatchPlan
     unsigned* d_counters = nullptr;
     size_t ws_bytes = 0, tab_bytes = 0;
     int minb = 1, grab = 1, grid = 0;
+    unsigned max_polls = BARRIER_MAX_POLLS, barrier_extra = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int device = 0;
@@ -280,6 +284,8 @@ template <typename T, int MINB> static int batch_launch(BatchPlan* P, const void
     for (int i = 0; i < 3; i++) A.nitems[i] = P->nitems[i];
     A.counters = P->d_counters;
     A.grab = P->grab;
+    A.max_polls = P->max_polls;
+    A.barrier_extra = P->barrier_extra;
     // work counters and barrier arrivals start at zero every execution (the
     // timeout flag, slot 6, is cleared only by gpufft_batch_plan_status)
     e = cudaMemsetAsync(P->d_counters, 0, 6 * sizeof(unsigned), s);
@@ -518,6 +524,13 @@ static void cache_store(const char* path, const std::string& key, int minb, int 
     f << "{\"key\": \"" << key << "\", \"minb\": " << minb << ", \"grab\": " << grab << ", \"ms\": " << ms << "}\n";
 }
 
+static long long total_coeffs(const BatchPlan* P)
+{
+    long long t = 0;
+    for (int np : P->n_powers) t += 1LL << np;
+    return t;
+}
+
 static int autotune(BatchPlan* P, const void* a, const void* b, void* c, const char* cache, cudaStream_t s)
 {
     const std::string key = tune_key(P);
@@ -528,9 +541,24 @@ static int autotune(BatchPlan* P, const void* a, const void* b, void* c, const c
         P->grab = gb;
         return GPUFFT_SUCCESS;
     }
-    cudaEvent_t e0, e1;
+    // the product is run about 28 times on the caller's buffers: c must not
+    // overlap a or b (the inputs would be overwritten between runs)
+    {
+        const size_t bytes = (size_t)(P->precision / 8) * (size_t)total_coeffs(P);
+        auto overlap = [bytes](const void* x, const void* y) {
+            const char* px = static_cast<const char*>(x);
+            const char* py = static_cast<const char*>(y);
+            return px < py + bytes && py < px + bytes;
+        };
+        if (overlap(c, a) || overlap(c, b)) return GPUFFT_ERROR_INVALID_VALUE;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
-        return set_cuda_error(cudaGetLastError());
+    {
+        const cudaError_t err = cudaGetLastError();
+        if (e0) cudaEventDestroy(e0);
+        return set_cuda_error(err);
+    }
     float best = 1e30f;
     int bmb = 1, bgb = 1;
     const int minbs[3] = {1, 2, 0};
@@ -546,7 +574,13 @@ static int autotune(BatchPlan* P, const void* a, const void* b, void* c, const c
             cudaEventRecord(e0, s);
             for (int r = 0; r < 3; r++) st |= batch_execute(P, a, b, c, s);
             cudaEventRecord(e1, s);
-            if (cudaEventSynchronize(e1) != cudaSuccess) return set_cuda_error(cudaGetLastError());
+            if (cudaEventSynchronize(e1) != cudaSuccess)
+            {
+                const cudaError_t err = cudaGetLastError();
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return set_cuda_error(err);
+            }
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
             if (!st && ms < best)
@@ -671,6 +705,15 @@ extern "C" int gpufft_batch_plan_info(gpufft_batch_plan plan, int* ctas_per_sm, 
     if (items_per_grab) *items_per_grab = P->grab;
     if (grid) *grid = P->grid;
     if (workspace_bytes) *workspace_bytes = (long long)P->ws_bytes;
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_batch_plan_set_barrier(gpufft_batch_plan plan, unsigned max_polls, unsigned extra_arrivals)
+{
+    if (!plan || max_polls < 1 || extra_arrivals > 1024) return GPUFFT_ERROR_INVALID_VALUE;
+    auto* P = reinterpret_cast<gfb::BatchPlan*>(plan);
+    P->max_polls = max_polls;
+    P->barrier_extra = extra_arrivals;
     return GPUFFT_SUCCESS;
 }
 

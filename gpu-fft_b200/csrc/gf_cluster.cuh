@@ -32,6 +32,8 @@
 
 #include "gf_engine.cuh"
 
+#include <atomic>
+
 #include <cooperative_groups.h>
 
 namespace gfb
@@ -246,12 +248,13 @@ __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) cl
 
 // Tiles at or below which the contiguous 12-stage passes run as clusters
 // (0: never). Set by gpufft_set_cluster_tiles.
-extern int g_cluster_max_tiles;
+extern std::atomic<int> g_cluster_max_tiles;
 
 inline bool cluster_ok(long long tiles)
 {
     // the grid (8 CTAs per tile) must stay within the 2^31 - 1 limit of gridDim.x
-    return tiles > 0 && tiles <= g_cluster_max_tiles && tiles <= 0x7fffffffLL / CL_CTAS;
+    return tiles > 0 && tiles <= g_cluster_max_tiles.load(std::memory_order_relaxed) &&
+           tiles <= 0x7fffffffLL / CL_CTAS;
 }
 
 template <typename T, int MODE>

@@ -476,9 +476,10 @@ extern "C" int gpufft_negacyclic_mul_f64_host(const double* a, const double* b, 
 //   device image, so every GPU on which the library's kernels are loaded holds
 //   it until the process exits.
 // * Host code may not use the array's name as a device address (on the host it
-//   names a host-side shadow). The device address is looked up with
-//   cudaGetSymbolAddress once per device, on the first call made on that
-//   device, with that device current; make that first call before any stream
+//   names a host-side shadow). Every call looks the device address up with
+//   cudaGetSymbolAddress for the current device (so the address stays right
+//   after a cudaDeviceReset); the first call on a device also loads the
+//   module's device image there, so make that first call before any stream
 //   capture.
 // * Rings whose one-product workspace exceeds the array (N > 2^20) are
 //   rejected with GPUFFT_ERROR_WORKSPACE. Larger batches run in more waves.
@@ -487,8 +488,6 @@ extern "C" int gpufft_negacyclic_mul_f64_host(const double* a, const double* b, 
 //   overlaps on the GPU (different streams, or different host threads without
 //   ordering) race on the array: serialise them.
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 namespace gfb
 {
 constexpr size_t NOALLOC_SCRATCH_BYTES = 16ull << 20;
@@ -496,21 +495,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 static int noalloc_scratch(void** out)
 {
-    static std::mutex mu;
-    static void* addr[64] = {nullptr};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    // looked up on every call (a cheap runtime query, no allocation): the
+    // address stays right across cudaDeviceReset, which reloads this module's
+    // device image and may move the array
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return set_cuda_error(e);
-    if (dev < 0 || dev >= 64) return set_cuda_error(cudaErrorInvalidDevice);
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev])
-    {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return set_cuda_error(e);
-        addr[dev] = p;
-    }
-    *out = addr[dev];
+    *out = p;
     return GPUFFT_SUCCESS;
 }
 } // namespace gfb

@@ -4,11 +4,24 @@
 #include "gf_split.cuh"
 #include "gf_pipe.cuh"
 
+#include <atomic>
 #include <map>
 #include <vector>
 
 namespace gfb
 {
+// FP32 split products of rings N = 2^14 .. 2^16 with at most six limbs run
+// their contiguous stages in split_tile_kernel (1, the default) or in the
+// five-kernel chain of pass kernels and split_groups (0). Both give the same
+// integers; set by gpufft_set_split_tile. The tile kernel's bulk copies need a
+// 16-byte aligned workspace; others take the chain.
+static std::atomic<int> g_split_tile{1};
+
+static bool split_tile_ok(int m, int k)
+{
+    return g_split_tile.load(std::memory_order_relaxed) != 0 && m > EBITS && m - SPLIT_TILE_LT <= SPLIT_COL_MAX &&
+           k <= SPLIT_TILE_MAXK;
+}
 
 // --------------------------------------------------------------------------
 // host side
@@ -195,6 +208,47 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
             }
         }
         long long ctas = 0;
+        if constexpr (F32)
+        {
+            if (split_tile_ok(m, k) && (reinterpret_cast<uintptr_t>(ws) & 15) == 0)
+            {
+                // column kernels for the first / last m - 11 stages around the
+                // tile kernel's eleven contiguous stages of every limb and group
+                const int L0 = m - SPLIT_TILE_LT;
+                A.geo = PassGeo{};
+                A.geo.m = m;
+                int st;
+                {
+                    const long long threads = 2 * wv * (M >> L0);
+                    const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
+                    GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * sizeof(cx<T>)), s,
+                             "split_fwd0_col<f32,L%d,k%d>", L0, k);
+                    st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+                        return dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
+                            split_fwd0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
+                            return check_launch();
+                        });
+                    });
+                }
+                if (st) return st;
+                st = launch_split_tile(k, A, wv * (M >> SPLIT_TILE_LT), s);
+                if (st) return st;
+                {
+                    const long long threads = wv * (M >> L0);
+                    const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
+                    GF_TRACE(tr, (double)wv * M * ((2 * k - 1) * sizeof(cx<T>) + 2 * 8), s,
+                             "split_inv0_col<f32,L%d,k%d>", L0, k);
+                    st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+                        return dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
+                            split_inv0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
+                            return check_launch();
+                        });
+                    });
+                }
+                if (st) return st;
+                continue;
+            }
+        }
         // rings with one pass (FP64 only here) run a zero-stage column form
         // (digits, fold, twist) around that single contiguous pass
         const int L0 = p.np == 1 ? 0 : p.L[0];
@@ -336,6 +390,12 @@ static int split_mul_host(const int32_t* a, const int32_t* b, int64_t* c, int n_
 }
 
 } // namespace gfb
+
+extern "C" int gpufft_set_split_tile(int on)
+{
+    if (on < 0) return gfb::g_split_tile.load();
+    return gfb::g_split_tile.exchange(on ? 1 : 0);
+}
 
 extern "C" int gpufft_split_plan(int n_power, int input_bits, int non_negative, int* limb_bits, int* num_limbs)
 {

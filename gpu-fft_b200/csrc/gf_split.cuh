@@ -618,6 +618,13 @@ template <int L, bool SINGLE, int K> static int launch_mid_k(const SplitArgs& a,
     return launch_split(split_mid<L, SINGLE, K>, done, a, ctas, s);
 }
 
+// The split product's contiguous stages of every limb and limb group on
+// 2^SPLIT_TILE_LT-point tiles held in shared memory (gf_split_tile.cuh), for
+// up to SPLIT_TILE_MAXK limbs; compiled in gf_split_tile.cu.
+constexpr int SPLIT_TILE_LT = 11;
+constexpr int SPLIT_TILE_MAXK = 5;
+int launch_split_tile(int k, const SplitArgs& a, long long tiles, cudaStream_t s);
+
 // one-kernel products for rings N <= 8192 (transform length 2^L, L = 1..12),
 // compiled in separate translation units by L range
 int launch_split_single_lo(int L, const SplitArgs& a, long long ctas, cudaStream_t s);  // L 1..6

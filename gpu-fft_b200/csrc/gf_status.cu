@@ -7,6 +7,8 @@
 // entry point returns GPUFFT_ERROR_CUDA; the C++ drop-in rethrows it.
 #include "gf_common.cuh"
 
+#include <atomic>
+
 namespace
 {
 thread_local int g_last_cuda_error = 0;
@@ -17,7 +19,7 @@ namespace gfb
 
 // Contiguous 12-stage passes over at most this many 4096-point tiles run as
 // thread-block clusters (gf_cluster.cuh); 0 disables them.
-int g_cluster_max_tiles = 64;
+std::atomic<int> g_cluster_max_tiles{64};
 int set_cuda_error(cudaError_t e)
 {
     g_last_cuda_error = (int)e;
@@ -192,7 +194,6 @@ extern "C" int gpufft_version(void) { return 100; }
 
 extern "C" int gpufft_set_cluster_tiles(int max_tiles)
 {
-    const int prev = gfb::g_cluster_max_tiles;
-    if (max_tiles >= 0) gfb::g_cluster_max_tiles = max_tiles;
-    return prev;
+    if (max_tiles < 0) return gfb::g_cluster_max_tiles.load(std::memory_order_relaxed);
+    return gfb::g_cluster_max_tiles.exchange(max_tiles, std::memory_order_relaxed);
 }

@@ -67,8 +67,8 @@ int gpufft_trace_collect(int max_rows, char* names, int name_len, double* total_
  * 4096 points (small batches: N = 2^13..2^23 with few products) spread each
  * tile over a cluster of 8 CTAs instead of one CTA; results are bit-identical
  * either way. max_tiles = 0 disables the cluster form; a negative value only
- * queries. Returns the previous limit (default 64). Process-wide; not
- * synchronised with concurrent calls. */
+ * queries. Returns the previous limit (default 64). Process-wide (an atomic
+ * setting: calls on other threads see either the old or the new limit). */
 int gpufft_set_cluster_tiles(int max_tiles);
 
 /* The cudaError_t of the last GPUFFT_ERROR_CUDA raised on this host thread. */
@@ -266,7 +266,8 @@ int gpufft_batch_plan_run(gpufft_batch_plan plan, const void* a, const void* b, 
  * launch with 1 or 2 CTAs per SM and 1, 2 or 4 work items per grab, and the
  * per-class fused chains (reported as 0 CTAs per SM by _info). cache_path (may
  * be NULL) is a JSON-lines file of earlier results keyed by GPU, driver,
- * precision and size histogram. */
+ * precision and size histogram. The candidates run on the caller's buffers
+ * about 28 times, so c must not overlap a or b (GPUFFT_ERROR_INVALID_VALUE). */
 int gpufft_batch_plan_autotune(gpufft_batch_plan plan, const void* a, const void* b, void* c,
                                const char* cache_path, gpufft_stream_t stream);
 /* Choose the execution mode by hand: ctas_per_sm 1 or 2 (persistent launch,
@@ -281,6 +282,13 @@ int gpufft_batch_plan_info(gpufft_batch_plan plan, int* ctas_per_sm, int* items_
                            long long* workspace_bytes);
 /* Reads and clears the plan's barrier-timeout flag (synchronous). */
 int gpufft_batch_plan_status(gpufft_batch_plan plan, int* barrier_timeouts);
+/* The persistent launch's grid barriers give up after max_polls polls of
+ * about 64 ns each (default 2^26, several seconds) and set the timeout flag.
+ * extra_arrivals (default 0, at most 1024) raises every barrier's target above
+ * the grid size so that no barrier can complete: it exists only to make the
+ * bounded wait run out in a test (the results of such a run are meaningless;
+ * the kernel still returns and the context stays usable). */
+int gpufft_batch_plan_set_barrier(gpufft_batch_plan plan, unsigned max_polls, unsigned extra_arrivals);
 int gpufft_batch_plan_destroy(gpufft_batch_plan plan);
 
 /* Allocation-free gpufft_negacyclic_mul_f64, for callers that cannot call
@@ -288,7 +296,8 @@ int gpufft_batch_plan_destroy(gpufft_batch_plan plan);
  * hosts that own every device allocation, processes that must not grow their
  * device footprint after start-up). No reference counterpart. Scratch is a
  * 16 MiB library-owned device array that every GPU loading the library holds
- * until exit; the first call on each device looks up its address, so make it
+ * until exit; every call looks up its address on the current device (the
+ * first call there also loads the module), so make the first call on a device
  * before any stream capture. Rings with N > 2^20 return GPUFFT_ERROR_WORKSPACE.
  * All calls share the array: calls that overlap on the GPU race on it. */
 int gpufft_negacyclic_mul_f64_noalloc(const double* a, const double* b, double* c, int n_power, int batch,
@@ -308,12 +317,36 @@ size_t gpufft_negacyclic_mul_split_workspace_bytes(int n_power, int batch, int n
  * int32 coefficients with |x| < 2^input_bits, N = 2^n_power in [4, 2^22].
  * Limbs: limb_bits/num_limbs, or 0/0 for the plan of gpufft_split_plan.
  * `tables` is the f32 native twiddle block (gpufft_ffnt_make_tables_f32).
- * max_error (device pointer, may be NULL) receives the largest distance of a
- * limb-group value to its nearest integer; the result is exact when < 0.5. */
+ * max_error (device pointer, may be NULL; the call zeroes it first) receives
+ * the largest distance of any limb-group value to its nearest integer.
+ *
+ * What max_error certifies. Every result coefficient is exact when the
+ * floating-point error of every limb-group value is below 0.5. max_error
+ * measures the distance to the NEAREST integer, so it detects errors up to
+ * 0.5 but does not prove their absence: a value whose error exceeded 0.5 would
+ * sit near a wrong integer and could report a small distance. A worst-case
+ * (a-priori) bound for FP32 transforms of these lengths is orders of magnitude
+ * above 0.5, so exactness is statistical: the limb plan (gpufft_split_plan)
+ * keeps the predicted largest error at or below 0.2, from an error model
+ * calibrated on measured limb products, and the measured max_error on uniform
+ * 24-bit data is about 0.13 at N = 2^16 and 0.22 at N = 2^17. Group values
+ * above 2^22 report 1.0 (not certified), a timed-out internal wait reports
+ * +inf (see gpufft_split_wait_timeouts). */
 int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* b, int64_t* c, int n_power, int batch,
                                     int input_bits, int non_negative, int limb_bits, int num_limbs,
                                     const void* tables, void* workspace, size_t workspace_bytes,
                                     float* max_error, gpufft_stream_t stream);
+/* Rings N = 2^14 .. 2^16 with at most six limbs (and a 16-byte aligned
+ * workspace) run the contiguous stages of every limb and limb group in one
+ * persistent kernel that keeps a product
+ * tile's limb spectra in shared memory (on = 1, the default), or in the chain
+ * of separate pass and group-sum kernels (on = 0); the integers are the same.
+ * A negative value only queries. Returns the previous setting. Process-wide. */
+int gpufft_set_split_tile(int on);
+/* Waits of that kernel on its bulk copies are bounded (2 s); a wait that runs
+ * out makes the call report max_error = +inf and is counted here. Reads the
+ * count (synchronous) and clears it when `clear` is nonzero. */
+int gpufft_split_wait_timeouts(unsigned* count, int clear);
 /* The same exact product with FP64 transforms, N = 2^2 .. 2^17 (no reference
  * counterpart). Its limb plan uses the FP64 error model, so it needs far fewer
  * limbs (two 12-bit limbs for 24-bit coefficients at N = 2^16). `tables` is the

@@ -65,7 +65,7 @@ def test_batch_matches_per_size_launches(gf, O, dev, dtype):
     plan.close()
 
 
-def test_batch_4096_mixed_sizes_graph_and_autotune(gf, dev):
+def test_batch_4096_mixed_sizes_graph_and_autotune(gf, O, dev):
     # the full mixed workload: 4096 requests, ring sizes log-uniform over 2^10..2^17, FP64,
     # one persistent launch captured in a CUDA graph, autotuned launch shape
     rng = np.random.default_rng(4)
@@ -74,7 +74,25 @@ def test_batch_4096_mixed_sizes_graph_and_autotune(gf, dev):
     g = torch.Generator(device=dev).manual_seed(4)
     a = torch.randint(-(1 << 15), 1 << 15, (plan.total,), device=dev, generator=g).double()
     b = torch.randint(-(1 << 15), 1 << 15, (plan.total,), device=dev, generator=g).double()
+    plan.set_shape(1, 1)  # the persistent launch
     c0 = plan.execute(a, b)
+    # identical to one gpufft_negacyclic_mul_f64 call per ring size on the same data
+    got = plan.unpack(c0)
+    for np_ in sorted(set(n_powers)):
+        idx = [i for i, n in enumerate(n_powers) if n == np_]
+        o0 = int(min(plan.offsets[i] for i in idx))
+        n = 1 << np_
+        ref = gf.negacyclic_mul(a[o0:o0 + len(idx) * n].view(len(idx), n), b[o0:o0 + len(idx) * n].view(len(idx), n))
+        assert torch.equal(c0[o0:o0 + len(idx) * n].view(len(idx), n), ref), np_
+    # |c| < 2^47: exact against the __int128 product on sampled coefficients
+    for i in rng.choice(len(n_powers), 12, replace=False):
+        n = 1 << n_powers[i]
+        o = int(plan.offsets[i])
+        ai = a[o:o + n].cpu().numpy().astype(np.int64)
+        bi = b[o:o + n].cpu().numpy().astype(np.int64)
+        idx = np.sort(rng.choice(n, 64, replace=False)).astype(np.int32)
+        assert np.array_equal(np.rint(got[i].cpu().numpy()[idx]).astype(np.int64),
+                              O.wrap64(O.negacyclic_coeffs(ai, bi, idx)))
     with tempfile.TemporaryDirectory() as d:
         cache = os.path.join(d, "tune.jsonl")
         info = plan.autotune(a, b, torch.empty_like(a), cache)
@@ -129,4 +147,40 @@ def test_split_batch_exact_and_graph(gf, O, dev):
     s.synchronize()
     assert torch.equal(c2, c)
     assert float(err2.item()) == float(err.item())
+    plan.close()
+
+
+def test_batch_barrier_timeout_is_reported(gf, dev):
+    # the persistent launch's grid barriers are bounded waits: with a target
+    # that no barrier can reach (extra arrivals) and a short poll limit, every
+    # barrier gives up, the kernel returns, the plan reports the timeout, and
+    # the context stays usable -- the same plan then runs normally again
+    rng = np.random.default_rng(46)
+    n_powers = [14, 15, 16, 12, 13, 16, 14, 15]
+    plan = gf.BatchPlan(n_powers, torch.float64)
+    a = torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, plan.total).astype(np.float64)).to(dev)
+    b = torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, plan.total).astype(np.float64)).to(dev)
+    plan.set_shape(1, 1)
+    ref = plan.execute(a, b)
+    torch.cuda.synchronize()
+    assert plan.status() == 0
+    plan.set_barrier(max_polls=4096, extra_arrivals=1)
+    plan.execute(a, b)
+    torch.cuda.synchronize()
+    assert plan.status() == 1
+    assert plan.status() == 0  # reading clears the flag
+    plan.set_barrier()  # defaults
+    again = plan.execute(a, b)
+    torch.cuda.synchronize()
+    assert plan.status() == 0
+    assert torch.equal(again, ref)
+    plan.close()
+
+
+def test_batch_autotune_rejects_aliased_output(gf, dev):
+    plan = gf.BatchPlan([12, 13], torch.float64)
+    a = torch.zeros(plan.total, dtype=torch.float64, device=dev)
+    b = torch.zeros_like(a)
+    with pytest.raises(gf.GpufftError):
+        plan.autotune(a, b, a)
     plan.close()

@@ -96,3 +96,50 @@ def test_c2c_and_r2r_match_reference_gpu(gf, O, R, dev, n_power):
         torch.cuda.synchronize()
         out.append(np.rint(rb.cpu().numpy()[: batch * M]))
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("n_power", [12, 13, 16, 18])
+def test_c2c_negacyclic_mode_matches_reference_gpu(gf, O, R, dev, n_power):
+    # GPU_FFT with reduction_poly = X_N_plus (twiddle index 2^s + g into an
+    # M-entry psi table, reference fft.cu:67-74): forward of 2 * batch vectors,
+    # then the inverse with the product, ours and the reference's on the same
+    # data and the same FFT<double>(M) tables. A product of integer vectors
+    # through the negacyclic transforms is the product mod X^M + 1: identical
+    # after rounding.
+    rng = np.random.default_rng(970 + n_power)
+    M = 1 << n_power
+    batch = 2
+    roots, inv_roots, ninv = O.fft_tables(M, "f64")
+    d_roots, d_inv = td(roots, dev), td(inv_roots, dev)
+    x = (rng.standard_normal((2 * batch, M)) + 1j * rng.standard_normal((2 * batch, M))).astype(np.complex128)
+    ints = rng.integers(-(1 << 10), 1 << 10, (2 * batch, M)).astype(np.complex128)
+    for data, exact in ((x, False), (ints, True)):
+        res, specs = [], []
+        for impl in ("ours", "ref"):
+            buf = td(data.ravel(), dev)
+            if impl == "ours":
+                f = gf.lib().gpufft_fft_c2c_f64
+                st = f(buf.data_ptr(), d_roots.data_ptr(), n_power, 0, 0, 0, 1.0, 0.0, 2 * batch, 0, None)
+                spec = buf.clone()
+                st |= f(buf.data_ptr(), d_inv.data_ptr(), n_power, 1, 0, 0, 1.0 / M, 0.0, batch, 1, None)
+            else:
+                st = R.ref_gpu_fft_c2c_f64(buf.data_ptr(), d_roots.data_ptr(), n_power, 0, 0, 1.0, 0.0, 2 * batch,
+                                           0, None)
+                spec = buf.clone()
+                st |= R.ref_gpu_fft_c2c_f64(buf.data_ptr(), d_inv.data_ptr(), n_power, 1, 0, 1.0 / M, 0.0, batch,
+                                            1, None)
+            assert st == 0
+            torch.cuda.synchronize()
+            specs.append(spec.cpu().numpy())
+            res.append(buf.cpu().numpy()[: batch * M])
+        assert np.linalg.norm(specs[0] - specs[1]) / np.linalg.norm(specs[1]) < 1e-13
+        assert np.linalg.norm(res[0] - res[1]) / np.linalg.norm(res[1]) < 1e-13
+        if exact:
+            assert np.array_equal(np.rint(res[0].real), np.rint(res[1].real))
+            assert np.array_equal(np.rint(res[0].imag), np.rint(res[1].imag))
+            # and it is the negacyclic product
+            a0 = ints[0].real.astype(np.int64)
+            b0 = ints[batch].real.astype(np.int64)
+            want = O.wrap64(O.schoolbook(a0, b0)) if M <= 4096 else None
+            if want is not None:
+                assert np.array_equal(np.rint(res[0][:M].real).astype(np.int64), want)

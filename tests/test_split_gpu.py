@@ -108,3 +108,39 @@ def test_split_f64_matches_f32_full_batch(gf, dev):
     c64 = gf.negacyclic_mul_split(a, b, input_bits=24, non_negative=True, precision="f64")
     c32 = gf.negacyclic_mul_split(a, b, input_bits=24, non_negative=True, precision="f32")
     assert torch.equal(c64, c32)
+
+
+@pytest.mark.parametrize("n_power,batch,bits,nonneg,ws_products", [
+    (16, 37, 24, True, 10), (15, 21, 24, True, 0), (14, 9, 16, False, 4), (16, 5, 12, False, 0)])
+def test_split_tile_matches_pass_chain(gf, O, dev, n_power, batch, bits, nonneg, ws_products):
+    # the shared-memory tile kernel and the five-kernel pass chain give the same
+    # integers (several limb plans; workspaces of a few products, so that waves
+    # and persistent-CTA tails are uneven), and both are exact on samples
+    rng = np.random.default_rng(5100 + n_power + batch)
+    n = 1 << n_power
+    lo = 0 if nonneg else -(1 << bits)
+    a = rng.integers(lo, 1 << bits, (batch, n)).astype(np.int32)
+    b = rng.integers(lo, 1 << bits, (batch, n)).astype(np.int32)
+    ta, tb = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    w, k = gf.split_plan(n_power, bits, nonneg)
+    ws = None
+    if ws_products:
+        per = int(gf.lib().gpufft_negacyclic_mul_split_workspace_bytes(n_power, 1, k))
+        ws = torch.empty(per * ws_products, dtype=torch.uint8, device=dev)
+    gf.split_wait_timeouts(clear=True)
+    prev = gf.set_split_tile(1)
+    try:
+        c1, e1 = gf.negacyclic_mul_split(ta, tb, input_bits=bits, non_negative=nonneg, workspace=ws,
+                                         return_error=True)
+        gf.set_split_tile(0)
+        c0, e0 = gf.negacyclic_mul_split(ta, tb, input_bits=bits, non_negative=nonneg, workspace=ws,
+                                         return_error=True)
+    finally:
+        gf.set_split_tile(prev)
+    assert float(e1.item()) < 0.5 and float(e0.item()) < 0.5
+    assert torch.equal(c1, c0)
+    assert gf.split_wait_timeouts(clear=True) == 0
+    idx = np.sort(rng.choice(n, 256, replace=False)).astype(np.int32)
+    got = c1.cpu().numpy()
+    for kk in (0, batch - 1):
+        assert np.array_equal(got[kk, idx], O.wrap64(O.negacyclic_coeffs(a[kk], b[kk], idx)))
