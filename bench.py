@@ -79,7 +79,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -195,24 +195,25 @@ def cpu_reference_error(n, samples=256):
     return float(np.max(np.abs(diff.astype(np.float64))))
 
 
-def cpu_reference_line(n, threads, reps=1):
-    """The reference's CPU product on the host cores: the bounded sample of
-    cpu_sample_count products (one per thread at a time), median of `reps`
-    repetitions; the same sample in the bench's cpu_baseline and in the
-    --impl reference arm."""
-    cnt = cpu_sample_count(n, threads)
-    vals = []
-    for _ in range(reps):
-        v, kind, cores = cpu_baseline_reference(n, cnt, threads)
-        vals.append(v)
-    err = cpu_reference_error(n)
-    return {"value": statistics.median(vals), "unit": "products/s", "cores": cores, "kind": kind,
-            "sample": f"{cnt} products of N={n} (2^{n.bit_length() - 1}), FFNT<double>::MULT, one product per "
-                      f"host thread at a time, median of {reps}",
-            "exact": False if err is None or err > 0 else True,
-            "max_abs_error_on_sample": err,
-            "note": "the reference's FP64 product is not exact at this size (results reach about 2^62, where "
-                    "an FP64 ulp is 2^10); the GPU line's split product is"}, cnt
+def cpu_baseline_subprocess(args):
+    """The cpu_baseline leg: the --impl reference arm itself (same code, same
+    sample, a fresh process without the GPU arm's threads), 3 timed steps after
+    one warm-up; its value is the median step."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--n-power", str(args.n_power),
+           "--batch", str(args.batch), "--steps", "3", "--warmup", "1"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env).stdout.strip().splitlines()
+        ref = json.loads(out[-1])
+    except (subprocess.SubprocessError, ValueError, IndexError) as exc:
+        return {"unavailable": f"reference CPU arm failed: {exc}"}
+    cb = dict(ref["cpu_baseline"])
+    cb["exact"] = ref.get("exact")
+    cb["max_abs_error_on_sample"] = ref.get("max_abs_error_on_sample")
+    cb["note"] = ("the reference's FP64 product is not exact at this size (results reach about 2^62, where an FP64 "
+                  "ulp is 2^10); the GPU line's split product is")
+    cb["how"] = "bench.py --impl reference --steps 3 --warmup 1 in a fresh process (median step)"
+    return cb
 
 
 def run_reference(args, rank, world):
@@ -985,7 +986,7 @@ def main():
     if rank == 0 and world == 1 and args.ref_gpu:
         line["ref_gpu"] = reference_gpu_arm(gf, a64, b64, n_power, batch, args, dev, torch)
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"], _ = cpu_reference_line(n, os.cpu_count() or 1, reps=3)
+        line["cpu_baseline"] = cpu_baseline_subprocess(args)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

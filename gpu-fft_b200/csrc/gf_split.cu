@@ -14,13 +14,15 @@ namespace gfb
 // their contiguous stages in split_tile_kernel (1, the default) or in the
 // five-kernel chain of pass kernels and split_groups (0). Both give the same
 // integers; set by gpufft_set_split_tile. The tile kernel's bulk copies need a
-// 16-byte aligned workspace; others take the chain.
+// 16-byte aligned workspace, and it needs a tile per SM; others take the chain.
 static std::atomic<int> g_split_tile{1};
 
-static bool split_tile_ok(int m, int k)
+// The tile kernel runs one persistent CTA per SM; a launch with fewer tiles
+// than SMs (a few products) leaves most of the GPU idle and takes the chain.
+static bool split_tile_ok(int m, int k, long long products)
 {
     return g_split_tile.load(std::memory_order_relaxed) != 0 && m > EBITS && m - SPLIT_TILE_LT <= SPLIT_COL_MAX &&
-           k <= SPLIT_TILE_MAXK;
+           k <= SPLIT_TILE_MAXK && (products << (m - SPLIT_TILE_LT)) >= (long long)sm_count();
 }
 
 // --------------------------------------------------------------------------
@@ -210,7 +212,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         long long ctas = 0;
         if constexpr (F32)
         {
-            if (split_tile_ok(m, k) && (reinterpret_cast<uintptr_t>(ws) & 15) == 0)
+            if (split_tile_ok(m, k, wv) && (reinterpret_cast<uintptr_t>(ws) & 15) == 0)
             {
                 // column kernels for the first / last m - 11 stages around the
                 // tile kernel's eleven contiguous stages of every limb and group
@@ -218,12 +220,25 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                 A.geo = PassGeo{};
                 A.geo.m = m;
                 int st;
+                if (L0 == SPLIT_COL_MAX)
+                {
+                    // 16-point columns: each column on two lanes (half the registers)
+                    const long long threads = 2 * (2 * wv * (M >> L0));
+                    const unsigned blocks = (unsigned)((threads + SPLIT_COL2_THREADS - 1) / SPLIT_COL2_THREADS);
+                    GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * sizeof(cx<T>)), s,
+                             "split_fwd0_col2<f32,L%d,k%d>", L0, k);
+                    st = dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
+                        split_fwd0_col2<SPLIT_COL_MAX, KK><<<blocks, SPLIT_COL2_THREADS, 0, s>>>(A);
+                        return check_launch();
+                    });
+                }
+                else
                 {
                     const long long threads = 2 * wv * (M >> L0);
                     const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
                     GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * sizeof(cx<T>)), s,
                              "split_fwd0_col<f32,L%d,k%d>", L0, k);
-                    st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+                    st = dispatch_int<1, SPLIT_COL_MAX - 1>(L0, [&]<int LL>() {
                         return dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
                             split_fwd0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
                             return check_launch();
@@ -233,12 +248,24 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                 if (st) return st;
                 st = launch_split_tile(k, A, wv * (M >> SPLIT_TILE_LT), s);
                 if (st) return st;
+                if (L0 == SPLIT_COL_MAX)
+                {
+                    const long long threads = 2 * (wv * (M >> L0));
+                    const unsigned blocks = (unsigned)((threads + SPLIT_COL2_THREADS - 1) / SPLIT_COL2_THREADS);
+                    GF_TRACE(tr, (double)wv * M * ((2 * k - 1) * sizeof(cx<T>) + 2 * 8), s,
+                             "split_inv0_col2<f32,L%d,k%d>", L0, k);
+                    st = dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
+                        split_inv0_col2<SPLIT_COL_MAX, KK><<<blocks, SPLIT_COL2_THREADS, 0, s>>>(A);
+                        return check_launch();
+                    });
+                }
+                else
                 {
                     const long long threads = wv * (M >> L0);
                     const unsigned blocks = (unsigned)((threads + SPLIT_COL_THREADS - 1) / SPLIT_COL_THREADS);
                     GF_TRACE(tr, (double)wv * M * ((2 * k - 1) * sizeof(cx<T>) + 2 * 8), s,
                              "split_inv0_col<f32,L%d,k%d>", L0, k);
-                    st = dispatch_int<1, SPLIT_COL_MAX>(L0, [&]<int LL>() {
+                    st = dispatch_int<1, SPLIT_COL_MAX - 1>(L0, [&]<int LL>() {
                         return dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
                             split_inv0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
                             return check_launch();

@@ -464,6 +464,178 @@ __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitA
     }
 }
 
+// Paired-lane column kernels for 2^L0-point columns (L0 >= 2): lanes l and
+// l ^ 16 of a warp share 16 columns, lane half hb = (l >> 4) & 1 holding rows
+// i = 2 m + hb (m < 2^(L0-1)). Every stage with span h >= 2 pairs rows of one
+// parity and runs in the thread (twiddle table[i >> (L0 - s)] = table[m >>
+// (L0 - s - 1)]); the span-1 stage pairs rows 2m and 2m+1 across the two
+// lanes through one register exchange (__shfl_xor_sync). Same butterflies,
+// twiddles and order as split_fwd0_col / split_inv0_col, so the same values, at
+// half the registers per thread.
+constexpr int SPLIT_COL2_THREADS = 128; // five CTAs per SM (forward), four (inverse)
+
+__device__ __forceinline__ cx<float> shfl16(cx<float> v)
+{
+    return mk<float>(__shfl_xor_sync(0xffffffffu, v.x, 16), __shfl_xor_sync(0xffffffffu, v.y, 16));
+}
+
+template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5) split_fwd0_col2(const SplitArgs a)
+{
+    constexpr int R = 1 << L0, H = R / 2;
+    const int m = a.geo.m;
+    const long long M = 1LL << m, C = M >> L0;
+    const long long idx = (long long)blockIdx.x * SPLIT_COL2_THREADS + threadIdx.x;
+    const int hb = (int)((idx >> 4) & 1);
+    const long long col = ((idx >> 5) << 4) + (idx & 15); // column over all (operand, product)
+    const long long c = col & (C - 1);
+    const long long bb = col >> (m - L0);
+    const bool ok = bb < 2 * a.W; // the grid covers whole warps; every lane joins the exchange
+    const long long op = bb >= a.W ? 1 : 0, p = ok ? bb - op * a.W : 0;
+    const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M + c;
+    long long v0[H], v1[H];
+    cx<float> tw[H];
+#pragma unroll
+    for (int q = 0; q < H; q++)
+    {
+        const long long i = 2 * q + hb;
+        v0[q] = ok ? (long long)__ldg(src + i * C) + a.voff : 0;
+        v1[q] = ok ? (long long)__ldg(src + i * C + M) + a.voff : 0;
+        tw[q] = ldg<float>(a.twist + c + i * C);
+    }
+    const int w = a.w;
+    const long long mask = (1LL << w) - 1;
+    const int half = 1 << (w - 1);
+    cx<float>* dst = a.spec + (op * K * a.W + p) * M + c;
+#pragma unroll
+    for (int l = 0; l < K; l++)
+    {
+        cx<float> x[H];
+#pragma unroll
+        for (int q = 0; q < H; q++)
+        {
+            int d0, d1;
+            if (l < K - 1)
+            {
+                d0 = (int)(v0[q] & mask) - half;
+                d1 = (int)(v1[q] & mask) - half;
+                v0[q] >>= w;
+                v1[q] >>= w;
+            }
+            else
+            {
+                d0 = (int)v0[q];
+                d1 = (int)v1[q];
+            }
+            x[q] = cmul<float>(mk<float>((float)d0, (float)d1), tw[q]);
+        }
+        // stages s = 0 .. L0-2 (span h = 2^(L0-1-s) >= 2): rows q and q + h/2 of this lane
+#pragma unroll
+        for (int s = 0; s < L0 - 1; s++)
+        {
+            const int hh = 1 << (L0 - 2 - s);
+#pragma unroll
+            for (int q = 0; q < H; q++)
+                if (!(q & hh)) ct_bfly<float>(x[q], x[q + hh], ldg<float>(a.roots + (q >> (L0 - 1 - s))));
+        }
+        // stage L0-1 (span 1): U = row 2q (half 0), V = row 2q+1 (half 1), table[q]
+#pragma unroll
+        for (int q = 0; q < H; q++)
+        {
+            const cx<float> wt = ldg<float>(a.roots + q);
+            const cx<float> mine = hb ? cmul<float>(x[q], wt) : x[q]; // half 1 sends V w, half 0 sends U
+            const cx<float> other = shfl16(mine);
+            x[q] = hb ? csub<float>(other, mine) : cadd<float>(mine, other);
+        }
+        if (ok)
+        {
+            cx<float>* d = dst + (long long)l * a.W * M;
+#pragma unroll
+            for (int q = 0; q < H; q++) d[(2 * q + hb) * C] = x[q];
+        }
+    }
+}
+
+template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4) split_inv0_col2(const SplitArgs a)
+{
+    constexpr int R = 1 << L0, H = R / 2;
+    const int m = a.geo.m;
+    const long long M = 1LL << m, C = M >> L0;
+    const long long idx = (long long)blockIdx.x * SPLIT_COL2_THREADS + threadIdx.x;
+    const int hb = (int)((idx >> 4) & 1);
+    const long long col = ((idx >> 5) << 4) + (idx & 15);
+    const long long c = col & (C - 1);
+    const long long p0 = col >> (m - L0);
+    const bool ok = p0 < a.W;
+    const long long p = ok ? p0 : 0;
+    cx<float> un[H];
+#pragma unroll
+    for (int q = 0; q < H; q++)
+    {
+        const cx<float> u = ldg<float>(a.untwist + c + (2 * q + hb) * C);
+        un[q] = mk<float>(u.x * a.scale, u.y * a.scale); // scale folded in: exact, scale is 2^-m
+    }
+    long long acc_lo[H], acc_hi[H];
+#pragma unroll
+    for (int q = 0; q < H; q++) acc_lo[q] = acc_hi[q] = 0;
+    float err = 0.f;
+    const cx<float>* src = a.group + p * M + c + hb * C;
+    const long long gstride = a.W * M;
+    cx<float> nx[H];
+#pragma unroll
+    for (int q = 0; q < H; q++) nx[q] = __ldcs(src + 2 * q * C);
+#pragma unroll 1
+    for (int s = 0; s < 2 * K - 1; s++)
+    {
+        cx<float> x[H];
+#pragma unroll
+        for (int q = 0; q < H; q++) x[q] = nx[q];
+        if (s + 1 < 2 * K - 1)
+        {
+#pragma unroll
+            for (int q = 0; q < H; q++) nx[q] = __ldcs(src + (s + 1) * gstride + 2 * q * C);
+        }
+        // stage L0-1 (span 1) first: U = row 2q (half 0), V = row 2q+1 (half 1), table[q]
+#pragma unroll
+        for (int q = 0; q < H; q++)
+        {
+            const cx<float> other = shfl16(x[q]);
+            x[q] = hb ? cmul<float>(csub<float>(other, x[q]), ldg<float>(a.inv_roots + q)) : cadd<float>(x[q], other);
+        }
+        // stages L0-2 .. 0 (span 2^(L0-1-st) >= 2), rows q and q + h/2 of this lane
+#pragma unroll
+        for (int st = L0 - 2; st >= 0; st--)
+        {
+            const int hh = 1 << (L0 - 2 - st);
+#pragma unroll
+            for (int q = 0; q < H; q++)
+                if (!(q & hh)) gs_bfly<float>(x[q], x[q + hh], ldg<float>(a.inv_roots + (q >> (L0 - 1 - st))));
+        }
+        const int sh = a.w * s;
+#pragma unroll
+        for (int q = 0; q < H; q++)
+        {
+            const cx<float> v = cmul<float>(x[q], un[q]);
+            const float rr = rintf(v.x), ri = rintf(v.y);
+            err = fmaxf(err, group_error(v, rr, ri));
+            acc_lo[q] += (long long)((unsigned long long)(long long)rr << sh);
+            acc_hi[q] += (long long)((unsigned long long)(long long)ri << sh);
+        }
+    }
+    if (ok)
+    {
+        int64_t* dst = a.c + p * 2 * M + c;
+#pragma unroll
+        for (int q = 0; q < H; q++)
+        {
+            const long long i = 2 * q + hb;
+            const long long j = c + i * C;
+            __stcs(reinterpret_cast<long long*>(dst + i * C), acc_lo[q] + uu_term(a, j, 2 * M));
+            __stcs(reinterpret_cast<long long*>(dst + i * C + M), acc_hi[q] + uu_term(a, j + M, 2 * M));
+        }
+    }
+    report_err(a.max_err, ok ? err : 0.f);
+}
+
 // FP32 columns of 8 points fit 128 registers: four CTAs (16 warps) per
 // SM keep more group loads in flight.
 template <typename T, int L0> constexpr int inv0_col_min_blocks() { return (sizeof(T) == 4 && L0 == 3) ? 4 : 1; }

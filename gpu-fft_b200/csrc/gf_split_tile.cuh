@@ -127,6 +127,23 @@ __device__ __forceinline__ void stage_w0(float4* dst, const cx<float>* __restric
     }
 }
 
+// Twiddles of the outer rounds (windows 7 and 3: stages u = 0 .. 7 of the
+// tile) use table[(T << u) + i] for i < 2^u only (window 7: all threads the
+// same 2^u entries; window 3: thread t the 2^(u-4) entries from i = (t >> 3)
+// 2^(u-4)). Staged as entry 2^u + i of a 256-entry buffer, every pair stays
+// 16-byte aligned.
+constexpr int W37_ENTRIES = 256;
+
+__device__ __forceinline__ void stage_w37(cx<float>* dst, const cx<float>* __restrict__ tw, long long T, int tid,
+                                          int nthreads)
+{
+    for (int idx = tid + 1; idx < W37_ENTRIES; idx += nthreads)
+    {
+        const int u = 31 - __clz(idx);
+        dst[idx] = ldg<float>(tw + (T << u) + (idx - (1 << u)));
+    }
+}
+
 // One round: the butterflies of e-bits [LO, HI) inside window W. Stage u of the
 // tile's eleven (e-bit q = 10 - u) pairs e with e + 2^q and uses
 // table[(T << u) + (e >> (q + 1))]; for register r (bit pb of r = q - W clear)
@@ -134,7 +151,8 @@ __device__ __forceinline__ void stage_w0(float4* dst, const cx<float>* __restric
 // 2^(3 - pb) consecutive entries, loaded first so their latencies overlap.
 template <bool FWD, int W, int LO, int HI>
 __device__ __forceinline__ void round(cx<float> (&x)[R], const cx<float>* __restrict__ tw, long long T, int eb,
-                                      bool vec, const float4* staged = nullptr, int t = 0)
+                                      bool vec, const float4* staged = nullptr, int t = 0,
+                                      const cx<float>* outer = nullptr)
 {
     constexpr int A = LO - W, RB = HI - LO;
     static_assert(A >= 0 && RB >= 1 && A + RB <= 4, "the round's bits lie in its window");
@@ -148,6 +166,29 @@ __device__ __forceinline__ void round(cx<float> (&x)[R], const cx<float>* __rest
         const int nt = 1 << (3 - pb);
         const cx<float>* p0 = tw + (T << u) + (eb >> (q + 1));
         cx<float>* wk = w + nt - 1;
+        if constexpr (W == 7 || W == 3)
+        {
+            if (outer)
+            {
+                // entries 2^u + i, i = (eb >> (q + 1)) = 0 (window 7) or (t >> 3) 2^(u-4) (window 3)
+                const cx<float>* q0 = outer + (1 << u) + (eb >> (q + 1));
+                if (nt >= 2)
+                {
+#pragma unroll
+                    for (int h = 0; h < nt; h += 2)
+                    {
+                        const float4 v = *reinterpret_cast<const float4*>(q0 + h);
+                        wk[h] = mk<float>(v.x, v.y);
+                        wk[h + 1] = mk<float>(v.z, v.w);
+                    }
+                }
+                else
+                {
+                    wk[0] = q0[0];
+                }
+                continue;
+            }
+        }
         if constexpr (W == 0 && LO == 0 && HI == 3)
         {
             if (staged)
@@ -208,14 +249,16 @@ template <int W> __device__ __forceinline__ void slot_store(const cx<float> (&x)
     for (int r = 0; r < R; r++) sl[ad(r)] = x[r];
 }
 
-constexpr int NTEAM = 4;        // teams of HT threads
-constexpr int NTT = NTEAM * HT; // 512 threads per CTA
+constexpr int NTEAM = 6;        // teams of HT threads (768 threads, 80 registers each)
+constexpr int NTT = NTEAM * HT; // threads per CTA
 
-// slots, the staged window-0 twiddles of the forward and of the inverse tile,
-// one mbarrier per slot, the queue counter and the teams' items
+// slots, the staged twiddles (window 0, then windows 7 and 3) of the forward
+// and of the inverse tile, one mbarrier per slot, the queue counter and the
+// teams' items
 constexpr size_t smem_bytes(int k)
 {
-    return (size_t)(2 * k) * SLOT * sizeof(float2) + 2 * (size_t)W0_PAIRS * sizeof(float4) + (size_t)(2 * k) * 8 + 64;
+    return (size_t)(2 * k) * SLOT * sizeof(float2) + 2 * (size_t)W0_PAIRS * sizeof(float4) +
+           2 * (size_t)W37_ENTRIES * sizeof(float2) + (size_t)(2 * k) * 8 + 64;
 }
 
 } // namespace stile
@@ -235,7 +278,9 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
     cx<float>* slot = reinterpret_cast<cx<float>*>(smraw);
     float4* twf = reinterpret_cast<float4*>(slot + NS * SLOT); // window-0 twiddles of the forward tile
     float4* twi = twf + W0_PAIRS;                             // ... and of the inverse tile
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(twi + W0_PAIRS);
+    cx<float>* tof = reinterpret_cast<cx<float>*>(twi + W0_PAIRS); // windows 7 and 3, forward tile
+    cx<float>* toi = tof + W37_ENTRIES;                             // ... inverse tile
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(toi + W37_ENTRIES);
     int* ctl = reinterpret_cast<int*>(bar + NS); // [0] queue counter, [4 + team] the team's current item
 
     const int tid = threadIdx.x;
@@ -258,7 +303,12 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
         fence_mbar_init();
         ctl[0] = 0;
     }
-    if (blockIdx.x < tiles) stage_w0(twf, a.roots, (long long)blockIdx.x & ((1LL << lg_tiles) - 1), tid, NTT, vec);
+    if (blockIdx.x < tiles)
+    {
+        const long long T0 = (long long)blockIdx.x & ((1LL << lg_tiles) - 1);
+        stage_w0(twf, a.roots, T0, tid, NTT, vec);
+        stage_w37(tof, a.roots, T0, tid, NTT);
+    }
     __syncthreads();
 
     auto issue = [&](long long tile, int tau) {
@@ -279,12 +329,12 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
         cx<float> x[R];
 #pragma unroll
         for (int r = 0; r < R; r++) x[r] = sl[t + (r << 7)]; // unpadded natural order, as copied
-        round<true, 7, 7, 11>(x, a.roots, T, ebase<7>(t), vec);
+        round<true, 7, 7, 11>(x, a.roots, T, ebase<7>(t), vec, nullptr, t, tof);
         bar_named(tbar, HT); // the team has read the natural order
         slot_store<7>(x, sl, a7);
         bar_named(tbar, HT);
         slot_load<3>(x, sl, a3);
-        round<true, 3, 3, 7>(x, a.roots, T, ebase<3>(t), vec);
+        round<true, 3, 3, 7>(x, a.roots, T, ebase<3>(t), vec, nullptr, t, tof);
         slot_store<3>(x, sl, a3); // the positions this thread read
         bar_named(tbar, HT);
         slot_load<0>(x, sl, a0);
@@ -305,7 +355,7 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
         slot_store<0>(x, sl, a0);
         bar_named(tbar, HT);
         slot_load<3>(x, sl, a3);
-        round<false, 3, 3, 7>(x, a.inv_roots, T, ebase<3>(t), vec);
+        round<false, 3, 3, 7>(x, a.inv_roots, T, ebase<3>(t), vec, nullptr, t, toi);
         slot_store<3>(x, sl, a3);
         bar_named(tbar, HT);
         slot_load<7>(x, sl, a7);
@@ -315,7 +365,7 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
             fence_proxy_async();
             issue(next, s);
         }
-        round<false, 7, 7, 11>(x, a.inv_roots, T, ebase<7>(t), vec);
+        round<false, 7, 7, 11>(x, a.inv_roots, T, ebase<7>(t), vec, nullptr, t, toi);
         cx<float>* dst = a.group + ((long long)s * a.W + p) * M + (T << LT) + t;
 #pragma unroll
         for (int r = 0; r < R; r++) dst[r << 7] = x[r];
@@ -365,13 +415,23 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
         {
             const float uscale = (float)(1 << a.ur);
 #pragma unroll 1
-            for (int i = 0; i < P / NTT; i++)
+            for (int e = tid; e < P; e += NTT)
             {
-                const int e = tid + NTT * i;
                 const int ad = ppos(e);
                 cx<float> v[NS];
 #pragma unroll
                 for (int tau = 0; tau < NS; tau++) v[tau] = slot[tau * SLOT + ad];
+                // A_i B_j accumulated with paired fused multiply-adds:
+                // (a.x, a.x) (b.x, b.y) + (a.y, a.y) (-b.y, b.x), the pairs formed
+                // once per limb
+                float2 ax[K], ay[K], bs[K];
+#pragma unroll
+                for (int l = 0; l < K; l++)
+                {
+                    ax[l] = make_float2(v[l].x, v[l].x);
+                    ay[l] = make_float2(v[l].y, v[l].y);
+                    bs[l] = make_float2(-v[K + l].y, v[K + l].x);
+                }
                 cx<float> acc[NG];
 #pragma unroll
                 for (int sg = 0; sg < NG; sg++)
@@ -379,7 +439,11 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
                     acc[sg] = mk<float>(0.f, 0.f);
 #pragma unroll
                     for (int i2 = 0; i2 < K; i2++)
-                        if (sg - i2 >= 0 && sg - i2 < K) acc[sg] = cadd<float>(acc[sg], cmul<float>(v[i2], v[K + sg - i2]));
+                        if (sg - i2 >= 0 && sg - i2 < K)
+                        {
+                            acc[sg] = __ffma2_rn(ax[i2], v[K + sg - i2], acc[sg]);
+                            acc[sg] = __ffma2_rn(ay[i2], bs[sg - i2], acc[sg]);
+                        }
                 }
                 if (a.K)
                 {
@@ -425,7 +489,12 @@ __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitAr
         // of the next (the previous tile's inverse and this tile's forward items
         // are done)
         stage_w0(twi, a.inv_roots, T, tid, NTT, vec);
-        if (has_next) stage_w0(twf, a.roots, next & ((1LL << lg_tiles) - 1), tid, NTT, vec);
+        stage_w37(toi, a.inv_roots, T, tid, NTT);
+        if (has_next)
+        {
+            stage_w0(twf, a.roots, next & ((1LL << lg_tiles) - 1), tid, NTT, vec);
+            stage_w37(tof, a.roots, next & ((1LL << lg_tiles) - 1), tid, NTT);
+        }
         if (tid == 0) ctl[0] = 0; // the queue restarts
         __syncthreads();
         // slot NS-1 held a limb only: the next tile's copy can start now

@@ -336,8 +336,9 @@ int gpufft_negacyclic_mul_split_f32(const int32_t* a, const int32_t* b, int64_t*
                                     int input_bits, int non_negative, int limb_bits, int num_limbs,
                                     const void* tables, void* workspace, size_t workspace_bytes,
                                     float* max_error, gpufft_stream_t stream);
-/* Rings N = 2^14 .. 2^16 with at most six limbs (and a 16-byte aligned
- * workspace) run the contiguous stages of every limb and limb group in one
+/* Rings N = 2^14 .. 2^16 with at most five limbs (with a 16-byte aligned
+ * workspace, and at least one 2048-point tile per SM per wave: 10 products at
+ * N = 2^16) run the contiguous stages of every limb and limb group in one
  * persistent kernel that keeps a product
  * tile's limb spectra in shared memory (on = 1, the default), or in the chain
  * of separate pass and group-sum kernels (on = 0); the integers are the same.

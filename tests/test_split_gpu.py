@@ -110,12 +110,14 @@ def test_split_f64_matches_f32_full_batch(gf, dev):
     assert torch.equal(c64, c32)
 
 
-@pytest.mark.parametrize("n_power,batch,bits,nonneg,ws_products", [
-    (16, 37, 24, True, 10), (15, 21, 24, True, 0), (14, 9, 16, False, 4), (16, 5, 12, False, 0)])
-def test_split_tile_matches_pass_chain(gf, O, dev, n_power, batch, bits, nonneg, ws_products):
+@pytest.mark.parametrize("n_power,batch,bits,nonneg,ws_products,tiled", [
+    (16, 37, 24, True, 10, True), (15, 21, 24, True, 0, True), (14, 48, 16, False, 40, True),
+    (16, 12, 12, False, 0, True), (16, 3, 24, True, 0, False)])
+def test_split_tile_matches_pass_chain(gf, O, dev, n_power, batch, bits, nonneg, ws_products, tiled):
     # the shared-memory tile kernel and the five-kernel pass chain give the same
     # integers (several limb plans; workspaces of a few products, so that waves
-    # and persistent-CTA tails are uneven), and both are exact on samples
+    # and persistent-CTA tails are uneven), and both are exact on samples; a
+    # launch with fewer tiles than SMs (3 products) takes the chain
     rng = np.random.default_rng(5100 + n_power + batch)
     n = 1 << n_power
     lo = 0 if nonneg else -(1 << bits)
@@ -130,8 +132,12 @@ def test_split_tile_matches_pass_chain(gf, O, dev, n_power, batch, bits, nonneg,
     gf.split_wait_timeouts(clear=True)
     prev = gf.set_split_tile(1)
     try:
+        gf.trace_enable(True)
         c1, e1 = gf.negacyclic_mul_split(ta, tb, input_bits=bits, non_negative=nonneg, workspace=ws,
                                          return_error=True)
+        gf.trace_enable(False)
+        names = [r["kernel"] for r in gf.trace_collect()]
+        assert any(nm.startswith("split_tile") for nm in names) == tiled, names
         gf.set_split_tile(0)
         c0, e0 = gf.negacyclic_mul_split(ta, tb, input_bits=bits, non_negative=nonneg, workspace=ws,
                                          return_error=True)

@@ -312,3 +312,38 @@ def test_staged_window0_twiddles(m, T):
     for j in range(7):
         addrs = [j * HT + t for t in range(32)]
         assert addrs == list(range(addrs[0], addrs[0] + 32))
+
+
+def stage_w37(tab, T):
+    """stage_w37: entry 2^u + i = table[(T << u) + i], u = 0 .. 7, i < 2^u."""
+    dst = [None] * 256
+    for idx in range(1, 256):
+        u = idx.bit_length() - 1
+        src = (T << u) + (idx - (1 << u))
+        assert 0 <= src < len(tab)
+        dst[idx] = tab[src]
+    return dst
+
+
+@pytest.mark.parametrize("m,T", [(15, 0), (15, 15), (14, 7), (13, 2)])
+def test_staged_outer_twiddles(m, T):
+    """The window-7 and window-3 rounds read from the staged buffer exactly the
+    entries they read from the table, and their paired (16-byte) reads are
+    aligned."""
+    M = 1 << m
+    tab = np.arange(M // 2) + 0j
+    st = stage_w37(tab, T)
+    for w in (7, 3):
+        for t in range(HT):
+            eb = ebase(w, t)
+            for pb in range(4):
+                q = w + pb
+                u = LT - 1 - q
+                nt = 1 << (3 - pb)
+                base_tab = (T << u) + (eb >> (q + 1))
+                base_st = (1 << u) + (eb >> (q + 1))
+                assert base_st + nt <= 256
+                if nt >= 2:
+                    assert base_st % 2 == 0
+                for h in range(nt):
+                    assert st[base_st + h] == tab[base_tab + h]
