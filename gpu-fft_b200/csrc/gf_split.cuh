@@ -474,6 +474,11 @@ __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitA
 // half the registers per thread.
 constexpr int SPLIT_COL2_THREADS = 128; // five CTAs per SM (forward), four (inverse)
 
+__device__ __forceinline__ void prefetch_l2(const void* p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ cx<float> shfl16(cx<float> v)
 {
     return mk<float>(__shfl_xor_sync(0xffffffffu, v.x, 16), __shfl_xor_sync(0xffffffffu, v.y, 16));
@@ -583,12 +588,25 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4
     cx<float> nx[H];
 #pragma unroll
     for (int q = 0; q < H; q++) nx[q] = __ldcs(src + 2 * q * C);
+    // group s + 1 is loaded into registers while group s is transformed, and
+    // group s + 2 is prefetched into L2 (more bytes in flight than the
+    // registers could hold)
+    if (2 * K - 1 > 1)
+    {
+#pragma unroll
+        for (int q = 0; q < H; q++) prefetch_l2(src + gstride + 2 * q * C);
+    }
 #pragma unroll 1
     for (int s = 0; s < 2 * K - 1; s++)
     {
         cx<float> x[H];
 #pragma unroll
         for (int q = 0; q < H; q++) x[q] = nx[q];
+        if (s + 2 < 2 * K - 1)
+        {
+#pragma unroll
+            for (int q = 0; q < H; q++) prefetch_l2(src + (s + 2) * gstride + 2 * q * C);
+        }
         if (s + 1 < 2 * K - 1)
         {
 #pragma unroll
