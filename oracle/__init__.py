@@ -34,7 +34,8 @@ _c_int = ctypes.c_int
 
 def build(ref: bool = True) -> None:
     """Compile liboracle.so (and the reference CPU build when its sources exist)."""
-    target = ["all"] if ref and os.path.isdir(os.environ.get("REF_DIR", "/root/reference")) else [
+    ref_dir = os.environ.get("REF_DIR", os.path.normpath(os.path.join(HERE, "..", "..", "reference")))
+    target = ["all", f"REF_DIR={ref_dir}"] if ref and os.path.isdir(ref_dir) else [
         os.path.join(HERE, "liboracle.so")]
     subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
 
