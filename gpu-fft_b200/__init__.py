@@ -145,6 +145,8 @@ def lib() -> ctypes.CDLL:
         L.gpufft_set_cluster_tiles.argtypes = [i]
         L.gpufft_set_cluster_tiles.restype = i
         L.gpufft_batch_plan_set_barrier.argtypes = [vp, ctypes.c_uint, ctypes.c_uint]
+        L.gpufft_set_f64_middle.argtypes = [i]
+        L.gpufft_set_f64_middle.restype = i
         L.gpufft_set_split_tile.argtypes = [i]
         L.gpufft_set_split_tile.restype = i
         L.gpufft_split_wait_timeouts.argtypes = [vp, i]
@@ -398,6 +400,12 @@ def negacyclic_mul_split(a, b, out=None, input_bits=None, non_negative=None, lim
 # ---------------------------------------------------------------------------
 # Per-kernel device-time tracing
 # ---------------------------------------------------------------------------
+def set_f64_middle(r8: int) -> int:
+    """FP64 products' middle pass on 512 threads x 8 points (1, the default) or
+    256 x 16 (0); identical values. A negative value queries."""
+    return int(lib().gpufft_set_f64_middle(int(r8)))
+
+
 def set_split_tile(on: int) -> int:
     """FP32 split products of rings 2^14..2^16 (up to five limbs) run their
     contiguous stages in the shared-memory tile kernel (1, the default) or in

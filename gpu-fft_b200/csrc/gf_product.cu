@@ -20,13 +20,17 @@
 // Twiddles come from gpufft_ffnt_make_tables_*, generated on the device with
 // sincospi in double precision (then rounded to float for the f32 path).
 #include "gf_fused.cuh"
+#include "gf_fused_r8.cuh"
+
+#include <atomic>
 
 namespace gfb
 {
 
 // ---------------------------------------------------------------------------
 // device twiddle tables:  [roots M/2 | inverse roots M/2 | twist M | untwist M | U M]
-// roots[i] = e^{+2 pi i bitrev_{m-1}(i) / M}, twist[j] = e^{+i pi j / N}, M = N/2
+// roots[i] = e^{+2 pi i bitrev_{m-1}(i) / M}, twist[j] = e^{+i pi j / N}, M = N/2;
+// roots[2j+1] = i roots[2j] exactly (the inverse roots are exact conjugates)
 // (the values of the reference's ReverseRootTable_ffnt / twist_table_ffnt,
 // fft_cpu.cu:251-297, 435-473, computed here in double precision).
 // U[r] is the FFNT spectrum of the all-ones polynomial u = 1 + X + ... + X^(N-1)
@@ -44,9 +48,20 @@ template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < H)
     {
-        const unsigned br = (m > 1) ? (__brev((unsigned)i) >> (33 - m)) : 0u;
+        // odd entries are exactly i times their even neighbour: bit reversal
+        // makes index 2j+1 the angle of 2j plus a quarter turn, and the table
+        // stores that relation exactly (kernels of the native products may
+        // load the even entry only and rotate it)
+        const long long ie = i & ~1LL;
+        const unsigned br = (m > 1) ? (__brev((unsigned)ie) >> (33 - m)) : 0u;
         double s, c;
         sincospi(2.0 * (double)br / (double)M, &s, &c);
+        if (i & 1)
+        {
+            const double t = c;
+            c = -s;
+            s = t;
+        }
         tab[i] = mk<T>((T)c, (T)s);
         tab[H + i] = mk<T>((T)c, (T)-s);
     }
@@ -91,6 +106,23 @@ static int launch_fused_shape(const FusedArgs<T>& a, long long ctas, cudaStream_
     return check_launch();
 }
 
+// The FP64 middle pass runs on 512 threads x 8 points per operand
+// (fused_r8_kernel, 1: the default) or in the engine's 256 x 16 form (0); the
+// values are identical. Set by gpufft_set_f64_middle.
+static std::atomic<int> g_f64_middle_r8{1};
+
+static int launch_fused_r8(const FusedArgs<double>& a, long long ctas, cudaStream_t s)
+{
+    static int done[64] = {0};
+    const size_t smem = r8::smem_bytes(sizeof(cx<double>));
+    int st = ensure_smem(fused_r8_kernel<double>, smem, done);
+    if (st) return st;
+    const double M = (double)(1LL << a.geo.m);
+    GF_TRACE(tr, (double)a.batch * M * 6.0 * sizeof(double), s, "fused_r8_kernel<f64,L12,middle>");
+    fused_r8_kernel<double><<<dim3((unsigned)ctas), dim3(r8::THREADS), smem, s>>>(a);
+    return check_launch();
+}
+
 template <typename T, bool SINGLE> static int launch_fused(const FusedArgs<T>& a, long long ctas, cudaStream_t s)
 {
     if (ctas <= 0) return GPUFFT_SUCCESS;
@@ -107,6 +139,10 @@ template <typename T, bool SINGLE> static int launch_fused(const FusedArgs<T>& a
         c.inv_table = a.inv_roots;
         c.m = a.geo.m;
         return launch_cluster_pass<T, CLM_FUSED>(c, ctas, a.batch, s);
+    }
+    if constexpr (!SINGLE && sizeof(T) == 8)
+    {
+        if (g_f64_middle_r8.load(std::memory_order_relaxed)) return launch_fused_r8(a, ctas, s);
     }
     if (!SINGLE) return launch_fused_shape<T, EBITS, false>(a, ctas, s);
     return dispatch_int<1, EBITS>(a.geo.m, [&]<int LL>() { return launch_fused_shape<T, LL, true>(a, ctas, s); });
@@ -330,6 +366,12 @@ template <typename T> static int make_tables(int n_power, void* tables, cudaStre
 }
 
 } // namespace gfb
+
+extern "C" int gpufft_set_f64_middle(int r8)
+{
+    if (r8 < 0) return gfb::g_f64_middle_r8.load();
+    return gfb::g_f64_middle_r8.exchange(r8 ? 1 : 0);
+}
 
 extern "C" size_t gpufft_ffnt_tables_count(int n_power)
 {

@@ -71,6 +71,13 @@ int gpufft_trace_collect(int max_rows, char* names, int name_len, double* total_
  * setting: calls on other threads see either the old or the new limit). */
 int gpufft_set_cluster_tiles(int max_tiles);
 
+/* The middle pass of the two-pass FP64 products (the last 12 forward stages of
+ * both operands, their product, the first 12 inverse stages of each 4096-point
+ * tile) runs on 512 threads of 8 points per operand (r8 = 1, the default) or
+ * on 256 threads of 16 (r8 = 0). The values are identical. A negative value
+ * only queries. Returns the previous setting. Process-wide (atomic). */
+int gpufft_set_f64_middle(int r8);
+
 /* The cudaError_t of the last GPUFFT_ERROR_CUDA raised on this host thread. */
 int gpufft_last_cuda_error(void);
 /* A static, human-readable string for a gpufft_status value. */
@@ -153,7 +160,9 @@ int gpufft_host_ffnt_tables_f64(int n, void* roots, void* inv_roots, void* twist
  * the transform of the all-ones polynomial (used by the split product; for
  * N > 8192 stored in that product's spectrum order, each block of 4096
  * entries permuted e -> (e >> 4) + 256 (e & 15)). All are computed on the
- * device with sincospi. */
+ * device with sincospi; each odd root is stored as exactly i times its even
+ * neighbour (bit reversal makes their angles a quarter turn apart), and the
+ * inverse roots as exact conjugates. */
 size_t gpufft_ffnt_tables_count(int n_power);
 int gpufft_ffnt_make_tables_f32(int n_power, void* tables, gpufft_stream_t stream);
 int gpufft_ffnt_make_tables_f64(int n_power, void* tables, gpufft_stream_t stream);
@@ -178,7 +187,9 @@ size_t gpufft_negacyclic_mul_workspace_bytes(int n_power, int batch, int precisi
 
 /* c[k] = a[k] * b[k] mod (X^N + 1) for k < batch, N = 2^n_power in [4, 2^22].
  * a, b, c: batch x N reals (row-major); c may alias a or b. `tables` is the
- * native twiddle block above. The output is not rounded (as GPU_FFNT). */
+ * native twiddle block above, as gpufft_ffnt_make_tables_* writes it (the
+ * kernels rely on its exact relations: roots[2j+1] = i roots[2j], inverse
+ * roots the exact conjugates). The output is not rounded (as GPU_FFNT). */
 int gpufft_negacyclic_mul_f32(const float* a, const float* b, float* c, int n_power, int batch,
                               const void* tables, void* workspace, size_t workspace_bytes,
                               gpufft_stream_t stream);

@@ -133,3 +133,34 @@ def test_cyclic_product_matches_dropin(gf, O, dev):
     gf.check(L.gpufft_fft_c2c_f64(buf.data_ptr(), d_i.data_ptr(), n_power, 1, 1, 0, 1.0 / M, 0.0, batch, 1, None), "i")
     ref = buf[: batch * M].cpu().view(batch, M)
     assert (torch.linalg.norm(got - ref) / torch.linalg.norm(ref)).item() < 1e-14
+
+
+@pytest.mark.parametrize("n_power,batch", [(14, 40), (16, 33), (17, 20), (20, 3)])
+def test_f64_middle_forms_identical(gf, O, dev, n_power, batch):
+    # the FP64 middle pass on 512 x 8 points (radix-8 rounds) and on 256 x 16
+    # (the engine's radix-16 rounds) runs the same butterflies: identical bits,
+    # for the negacyclic and the cyclic products; exact on sampled coefficients
+    rng = np.random.default_rng(880 + n_power)
+    n = 1 << n_power
+    a = torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, (batch, n)).astype(np.float64)).to(dev)
+    b = torch.from_numpy(rng.integers(-(1 << 15), 1 << 15, (batch, n)).astype(np.float64)).to(dev)
+    prev = gf.set_f64_middle(1)
+    try:
+        gf.set_cluster_tiles(0)  # the tiled middle pass, not its cluster form
+        c1 = gf.negacyclic_mul(a, b)
+        x = torch.complex(a, b)
+        y = torch.complex(b, a)
+        k1 = gf.cyclic_mul(x, y)
+        gf.set_f64_middle(0)
+        c0 = gf.negacyclic_mul(a, b)
+        k0 = gf.cyclic_mul(x, y)
+    finally:
+        gf.set_f64_middle(prev)
+        gf.set_cluster_tiles(64)
+    assert torch.equal(c1, c0)
+    assert torch.equal(k1, k0)
+    idx = np.sort(rng.choice(n, 64, replace=False)).astype(np.int32)
+    got = np.rint(c1[batch - 1].cpu().numpy()[idx]).astype(np.int64)
+    want = O.wrap64(O.negacyclic_coeffs(a[batch - 1].cpu().numpy().astype(np.int64),
+                                        b[batch - 1].cpu().numpy().astype(np.int64), idx))
+    assert np.array_equal(got, want)
