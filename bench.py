@@ -451,10 +451,12 @@ def time_path(step, host_step, a, b, c, hosts, args, stream, torch, barrier, max
 # replay, so this is the cold-cache figure). Both scale with the products per
 # launch, so traffic per launch = ratio x the kernel's tagged bytes per launch.
 NCU_TRAFFIC = {
+    # 64 products (1024 tiles): 168.8 MB read + 99.8 MB written of 318.8 MB tagged
+    "split_tile<k5>": (268.5 / 318.8, "ncu capture of a 64-product launch"),
+    # wave of 74 products (592 tiles): 78.1 MB read + 2.7 MB written of 116.4 MB tagged
+    "fused_r8_kernel<f64,L12,middle>": (80.9 / 116.4, "ncu capture of a 74-product wave"),
     # wave of 46 products (3680 CTAs): 120.8 MB read + 63.5 MB written of 241.2 MB tagged
     "pass_kernel<f32,fwd,L12,contiguous>": (184.3 / 241.2, "ncu capture of a 46-product wave"),
-    # wave of 74 products (592 CTAs): 78.2 MB read + 2.8 MB written of 116.4 MB tagged
-    "fused_kernel<f64,L12,middle>": (81.0 / 116.4, "ncu capture of a 74-product wave"),
 }
 
 
