@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-ref-gpu", dest="ref_gpu", action="store_false",
                    help="skip timing the reference's own GPU build beside ours (N = 1 only)")
+    p.add_argument("--check", default=None,
+                   help="(--impl reference) .npz of sampled GPU outputs to check against the exact product; "
+                        "written by the GPU arm for its cpu_baseline leg")
     return p.parse_args()
 
 
@@ -195,25 +198,55 @@ def cpu_reference_error(n, samples=256):
     return float(np.max(np.abs(diff.astype(np.float64))))
 
 
-def cpu_baseline_subprocess(args):
+def cpu_baseline_subprocess(args, check_path=None):
     """The cpu_baseline leg: the --impl reference arm itself (same code, same
     sample, a fresh process without the GPU arm's threads), 3 timed steps after
-    one warm-up; its value is the median step."""
+    one warm-up; its value is the median step. The same process checks the GPU
+    arm's sampled outputs (`check_path`) against the exact product and times the
+    reference's GPU build. Returns (cpu_baseline, the reference arm's line)."""
     cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--n-power", str(args.n_power),
            "--batch", str(args.batch), "--steps", "3", "--warmup", "1"]
+    if check_path:
+        cmd += ["--check", check_path]
+    if not args.ref_gpu:
+        cmd += ["--no-ref-gpu"]
     env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
     try:
-        out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env).stdout.strip().splitlines()
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=900, env=env).stdout.strip().splitlines()
         ref = json.loads(out[-1])
     except (subprocess.SubprocessError, ValueError, IndexError) as exc:
-        return {"unavailable": f"reference CPU arm failed: {exc}"}
+        return {"unavailable": f"reference CPU arm failed: {exc}"}, {}
     cb = dict(ref["cpu_baseline"])
     cb["exact"] = ref.get("exact")
     cb["max_abs_error_on_sample"] = ref.get("max_abs_error_on_sample")
     cb["note"] = ("the reference's FP64 product is not exact at this size (results reach about 2^62, where an FP64 "
                   "ulp is 2^10); the GPU line's split product is")
     cb["how"] = "bench.py --impl reference --steps 3 --warmup 1 in a fresh process (median step)"
-    return cb
+    return cb, ref
+
+
+def check_samples(path):
+    """Exactness of the GPU arm's sampled outputs: the first product of each
+    path at 64 seeded coefficient indices against the exact negacyclic product
+    (int64 wrap-around)."""
+    import numpy as np
+    import oracle as O
+    d = np.load(path)
+    idx = d["idx"].astype(np.int32)
+    want = O.wrap64(O.negacyclic_coeffs(d["a0"], d["b0"], idx))
+    res = {}
+    for k in d.files:
+        if not k.startswith("out_"):
+            continue
+        got = d[k]
+        if got.dtype != np.int64:
+            err = float(np.max(np.abs(got.astype(np.float64) - want.astype(np.float64))))
+            exact = bool(np.array_equal(np.rint(got).astype(np.int64), want))
+        else:
+            err = float(np.max(np.abs((got - want).astype(np.float64))))
+            exact = bool(np.array_equal(got, want))
+        res[k[4:]] = {"exact": exact, "max_abs_error": err}
+    return res
 
 
 def run_reference(args, rank, world):
@@ -243,88 +276,196 @@ def run_reference(args, rank, world):
                              "sample": f"{cnt} products of N=2^{args.n_power} per step, FFNT<double>::MULT, "
                                        "one product per host thread at a time"},
             "e2e": {"value": val, "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.check:
+        line["check"] = check_samples(args.check)
+    if args.ref_gpu:
+        line["ref_gpu"] = reference_gpu_cases(args)
+        if "unavailable" not in line["ref_gpu"]:
+            line["nvbench"] = run_nvbench(os.path.join(ROOT, "oracle", "_ref", "bench", NVBENCH_PROGRAM))
     print(json.dumps(line), flush=True)
 
 
-def reference_gpu_arm(gf, a64, b64, n_power, batch, args, dev, torch):
-    """The reference's own GPU path beside ours, on the same GPU and the same
-    FP64 inputs: its src/lib/fft.cu built for sm_100a (oracle/_ref, called
-    through its C++ API GPU_FFNT: forward of 2*batch, inverse with the product,
-    reference-format tables), this library's drop-in GPU_FFNT (the same two
-    calls) and its native FP64 and exact split products, at the workload's batch
-    and at batch 1 (the shape of the reference's own benchmark,
-    bench_gpu_ffnt_R_R_mult.cu). CUDA events around K steps after W warm-ups."""
-    import ctypes
+def events_ms(fn, args, torch, stream):
+    """Mean ms of fn() over K calls, CUDA events on `stream`, after W (>= 3) warm-ups."""
+    for _ in range(max(3, args.warmup)):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / args.steps
+
+
+def ffnt_product_calls(fn, bufs, tables, n_power, bt, status):
+    """The reference API's FFNT product as its benchmark bench_gpu_ffnt_R_R_mult.cu
+    forms it: GPU_FFNT forward of 2*bt rows, then GPU_FFNT inverse with the
+    product (mod_inverse 2/N) of bt rows. `fn` is a GPU_FFNT C entry point
+    (inout, temp, twist, roots, n_power, fft_type, mod_inverse re/im, batch, mult,
+    stream); the call statuses are appended to `status`."""
+    inout, temp = bufs
+    roots, inv_roots, twist, untwist = tables
+    h = (1 << n_power) // 2
+
+    def run():
+        st = fn(inout.data_ptr(), temp.data_ptr(), twist.data_ptr(), roots.data_ptr(), n_power, 0, 1.0, 0.0,
+                2 * bt, 0, None)
+        st |= fn(inout.data_ptr(), temp.data_ptr(), untwist.data_ptr(), inv_roots.data_ptr(), n_power, 1, 1.0 / h,
+                 0.0, bt, 1, None)
+        status.append(st)
+    return run
+
+
+REF_GPU_BATCHES = (None, 1)  # the workload's batch, and batch 1
+
+
+def ours_gpu_cases(gf, a64, b64, n_power, batch, args, dev, torch):
+    """This library's side of the comparison with the reference's GPU build on
+    the workload's inputs: the drop-in GPU_FFNT (the reference benchmark's two
+    calls on FFNT<double> tables from this library's host generator, bitwise
+    equal to the reference's), and the native FP64 and exact split products, at
+    the workload's batch and at batch 1. The --impl reference arm times the
+    reference's build the same way; the GPU arm divides the two."""
     import numpy as np
-    import oracle as O
-    R = O.ref_gpu()
-    if R is None:
-        return {"unavailable": "the reference's GPU build (oracle/_ref/libgpufft_ref_gpu.so) is absent"}
     n = 1 << n_power
     h = n // 2
-    roots, inv_roots, twist, untwist = [torch.from_numpy(np.ascontiguousarray(t)).to(dev)
-                                        for t in O.ffnt_tables(n, "f64")]
+    tables = [torch.from_numpy(np.ascontiguousarray(t)).to(dev) for t in gf.host_ffnt_tables(n, "f64")]
     L = gf.lib()
     stream = torch.cuda.current_stream()
-
-    def timed(fn):
-        for _ in range(max(3, args.warmup)):
-            fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / args.steps
-
-    out = {"timed": "CUDA events around K steps (each step: the two GPU_FFNT calls, or one product call)",
-           "tables": "reference-format FFNT<double> tables on the device", "cases": []}
-    for bt in (batch, 1):
+    cases = []
+    for bt in (batch if b is None else b for b in REF_GPU_BATCHES):
         inout = torch.cat([a64[:bt].reshape(-1), b64[:bt].reshape(-1)]).double().to(dev)
         temp = torch.empty(bt * h, dtype=torch.complex128, device=dev)
-        chk = {}
-
-        def two(fn, ok):
-            def run():
-                st = fn(inout.data_ptr(), temp.data_ptr(), twist.data_ptr(), roots.data_ptr(), n_power, 0, 1.0,
-                        0.0, 2 * bt, 0, None)
-                st |= fn(inout.data_ptr(), temp.data_ptr(), untwist.data_ptr(), inv_roots.data_ptr(), n_power, 1,
-                         1.0 / h, 0.0, bt, 1, None)
-                ok.append(st)
-            return run
-        ok_ref, ok_ours = [], []
-        ms_ref = timed(two(R.ref_gpu_ffnt_f64, ok_ref))
-        ms_drop = timed(two(L.gpufft_ffnt_f64, ok_ours))
-        # native products on the same inputs
+        status = []
+        ms_drop = events_ms(ffnt_product_calls(L.gpufft_ffnt_f64, (inout, temp), tables, n_power, bt, status),
+                            args, torch, stream)
         ad, bd = a64[:bt].double().to(dev), b64[:bt].double().to(dev)
         cd = torch.empty_like(ad)
         tf = gf.ffnt_tables(n_power, "f64", dev)
         ws = torch.empty(max(1, gf.negacyclic_mul_workspace_bytes(n_power, bt, 64)), dtype=torch.uint8, device=dev)
-        ms_f64 = timed(lambda: gf.negacyclic_mul(ad, bd, out=cd, tables=tf, workspace=ws))
+        ms_f64 = events_ms(lambda: gf.negacyclic_mul(ad, bd, out=cd, tables=tf, workspace=ws), args, torch, stream)
         ai, bi = a64[:bt].to(torch.int32).to(dev), b64[:bt].to(torch.int32).to(dev)
         ci = torch.empty((bt, n), dtype=torch.int64, device=dev)
         w, k = gf.split_plan(n_power, 24, True)
         t32 = gf.ffnt_tables(n_power, "f32", dev)
         wss = torch.empty(max(1, int(L.gpufft_negacyclic_mul_split_workspace_bytes(n_power, bt, k))),
                           dtype=torch.uint8, device=dev)
-        ms_split = timed(lambda: gf.negacyclic_mul_split(ai, bi, out=ci, input_bits=24, non_negative=True,
-                                                         limbs=(w, k), tables=t32, workspace=wss))
-        if any(ok_ref) or any(ok_ours):
-            return {"unavailable": f"a GPU_FFNT call failed (status {max(ok_ref + ok_ours)})"}
-        out["cases"].append({
-            "batch": bt, "ring_log2": n_power,
-            "ref_gpu_ms": ms_ref, "ref_gpu_value": bt / (ms_ref * 1e-3),
-            "ours_dropin_ms": ms_drop, "ours_dropin_value": bt / (ms_drop * 1e-3),
-            "ours_f64_ms": ms_f64, "ours_f64_value": bt / (ms_f64 * 1e-3),
-            "ours_split_ms": ms_split, "ours_split_value": bt / (ms_split * 1e-3),
-            "dropin_vs_ref": ms_ref / ms_drop, "f64_vs_ref": ms_ref / ms_f64, "split_vs_ref": ms_ref / ms_split})
+        ms_split = events_ms(lambda: gf.negacyclic_mul_split(ai, bi, out=ci, input_bits=24, non_negative=True,
+                                                             limbs=(w, k), tables=t32, workspace=wss),
+                             args, torch, stream)
+        if any(status):
+            return {"unavailable": f"a GPU_FFNT call failed (status {max(status)})"}
+        cases.append({"batch": bt, "ring_log2": n_power, "ours_dropin_ms": ms_drop, "ours_f64_ms": ms_f64,
+                      "ours_split_ms": ms_split})
         del inout, temp, ad, bd, cd, ws, ai, bi, ci, wss
         torch.cuda.empty_cache()
-    head = out["cases"][0]
-    out["ref_gpu_value"] = head["ref_gpu_value"]
-    out["unit"] = "products/s"
+    return {"cases": cases}
+
+
+def reference_gpu_cases(args):
+    """The reference's own GPU path on the workload's inputs: its src/lib/fft.cu
+    built unmodified for sm_100a (oracle/_ref), called through its C++ API
+    GPU_FFNT as its benchmark bench_gpu_ffnt_R_R_mult.cu does (forward of
+    2*batch, inverse with the product), on the reference's FFNT<double>
+    tables, at the workload's batch and at batch 1. CUDA events around K steps
+    after W warm-ups."""
+    try:
+        import torch
+    except ImportError:
+        return {"unavailable": "torch is not importable"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no GPU"}
+    import numpy as np
+    import oracle as O
+    R = O.ref_gpu()
+    if R is None:
+        return {"unavailable": "the reference's GPU build (oracle/_ref/libgpufft_ref_gpu.so) is absent"}
+    dev = torch.device("cuda", 0)
+    n_power, batch = args.n_power, args.batch
+    n = 1 << n_power
+    h = n // 2
+    a64, b64 = make_inputs(batch, n, 0)
+    tables = [torch.from_numpy(np.ascontiguousarray(t)).to(dev) for t in O.ffnt_tables(n, "f64")]
+    stream = torch.cuda.current_stream()
+    cases = []
+    for bt in (batch if b is None else b for b in REF_GPU_BATCHES):
+        inout = torch.cat([a64[:bt].reshape(-1), b64[:bt].reshape(-1)]).double().to(dev)
+        temp = torch.empty(bt * h, dtype=torch.complex128, device=dev)
+        status = []
+        ms = events_ms(ffnt_product_calls(R.ref_gpu_ffnt_f64, (inout, temp), tables, n_power, bt, status),
+                       args, torch, stream)
+        if any(status):
+            return {"unavailable": f"a reference GPU_FFNT call failed (status {max(status)})"}
+        cases.append({"batch": bt, "ring_log2": n_power, "ref_gpu_ms": ms, "ref_gpu_value": bt / (ms * 1e-3)})
+        del inout, temp
+    return {"cases": cases, "unit": "products/s",
+            "timed": "CUDA events around K steps (each step: the reference benchmark's two GPU_FFNT calls)"}
+
+
+def merge_gpu_cases(ours, ref):
+    """Per batch: both sides' ms and the reference's time over ours."""
+    if "cases" not in ours:
+        return ours
+    if not ref or "cases" not in ref:
+        return {"ours": ours, "reference": ref or {"unavailable": "the cpu_baseline leg did not run"}}
+    out = {"timed": "CUDA events around K steps on each side (the reference in the --impl reference arm's process)",
+           "tables": "FFNT<double> tables in the reference's format on the device", "unit": "products/s",
+           "cases": []}
+    for o, r in zip(ours["cases"], ref["cases"]):
+        bt = o["batch"]
+        c = {"batch": bt, "ring_log2": o["ring_log2"], "ref_gpu_ms": r["ref_gpu_ms"],
+             "ref_gpu_value": bt / (r["ref_gpu_ms"] * 1e-3)}
+        for k in ("dropin", "f64", "split"):
+            c[f"ours_{k}_ms"] = o[f"ours_{k}_ms"]
+            c[f"ours_{k}_value"] = bt / (o[f"ours_{k}_ms"] * 1e-3)
+            c[f"{k}_vs_ref"] = r["ref_gpu_ms"] / o[f"ours_{k}_ms"]
+        out["cases"].append(c)
+    out["ref_gpu_value"] = out["cases"][0]["ref_gpu_value"]
+    return out
+
+
+NVBENCH_PROGRAM = "gpu_ffnt_R_R_mult_benchmark"  # GPU_FFNT product, Ring Size LogN 12..23, Batch Count 1
+
+
+def run_nvbench(exe, timeout_s=180):
+    """One benchmark program on the nvbench-compatible harness (its own axes and
+    stopping rule: cold L2, CUDA events per sample, 1 s per state); returns the
+    harness's JSON."""
+    import tempfile
+    if not os.path.exists(exe):
+        return {"unavailable": f"{os.path.relpath(exe, ROOT)} is not built"}
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "states.json")
+        try:
+            subprocess.run([exe, "--json", out, "--md", os.devnull], check=True, timeout=timeout_s,
+                           capture_output=True)
+            with open(out) as f:
+                return json.load(f)
+        except (subprocess.SubprocessError, OSError, ValueError) as exc:
+            return {"unavailable": f"{os.path.basename(exe)} failed: {exc}"}
+
+
+def merge_nvbench(ours, ref):
+    """Per state of the program: both libraries' mean GPU time and the
+    reference's over ours."""
+    if "benchmarks" not in ours:
+        return {"ours": ours, "reference": ref}
+    if not ref or "benchmarks" not in ref:
+        return {"ours": ours, "reference": ref or {"unavailable": "the cpu_baseline leg did not run"}}
+    out = {"program": f"gpu-fft_b200/benchmark/bin/{NVBENCH_PROGRAM} (ours) and oracle/_ref/bench/{NVBENCH_PROGRAM} "
+                      "(the same source built on the reference's library)",
+           "timed": "cold L2 per sample, CUDA events, mean GPU time per state", "cases": []}
+    for bo, br in zip(ours["benchmarks"], ref["benchmarks"]):
+        for so, sr in zip(bo["states"], br["states"]):
+            c = {"benchmark": bo["name"], **{k.lower().replace(" ", "_"): v for k, v in so["axes"].items()}}
+            if "gpu_time_mean_s" in so and "gpu_time_mean_s" in sr:
+                c.update(ours_us=so["gpu_time_mean_s"] * 1e6, ref_us=sr["gpu_time_mean_s"] * 1e6,
+                         ref_over_ours=sr["gpu_time_mean_s"] / so["gpu_time_mean_s"])
+            else:
+                c.update(skipped=so.get("skipped") or sr.get("skipped"))
+            out["cases"].append(c)
     return out
 
 
@@ -968,27 +1109,35 @@ def main():
                       "dominant_kernel": {k: r["kroof"][k] for k in ("kernel", "achieved", "frac", "mean_launch_us",
                                                                      "share_of_step", "traffic")},
                       "e2e_value": world * batch / (r["ms_e2e"] * 1e-3)}
-    if rank == 0:
-        # exactness spot check of the first product: 64 sampled coefficients
+    ours_gpu = ours_nv = None
+    if rank == 0 and world == 1 and args.ref_gpu:
+        ours_gpu = ours_gpu_cases(gf, a64, b64, n_power, batch, args, dev, torch)
+        torch.cuda.synchronize()
+        ours_nv = run_nvbench(os.path.join(ROOT, "gpu-fft_b200", "benchmark", "bin", NVBENCH_PROGRAM))
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the cpu_baseline leg also checks the first product of each path at 64
+        # seeded coefficients against the exact product, and times the
+        # reference's GPU build
+        import tempfile
         import numpy as np
-        import oracle as O
         rng = np.random.default_rng(1)
         idx = np.sort(rng.choice(n, 64, replace=False)).astype(np.int32)
-        want = O.wrap64(O.negacyclic_coeffs(a64[0].numpy(), b64[0].numpy(), idx))
-        for name, r in results.items():
-            got = r["c"][0].numpy()[idx]
-            if got.dtype != np.int64:
-                err = float(np.max(np.abs(got.astype(np.float64) - want.astype(np.float64))))
-                exact = bool(np.array_equal(np.rint(got).astype(np.int64), want))
-            else:
-                err, exact = 0.0, bool(np.array_equal(got, want))
-            tgt = line if name == args.path else line[name]
-            tgt["exact_on_sample"] = exact
-            tgt["max_abs_error_on_sample"] = err
-    if rank == 0 and world == 1 and args.ref_gpu:
-        line["ref_gpu"] = reference_gpu_arm(gf, a64, b64, n_power, batch, args, dev, torch)
-    if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_subprocess(args)
+        with tempfile.TemporaryDirectory() as tmp:
+            chk = os.path.join(tmp, "samples.npz")
+            np.savez(chk, idx=idx, a0=a64[0].numpy(), b0=b64[0].numpy(),
+                     **{f"out_{name}": r["c"][0].numpy()[idx] for name, r in results.items()})
+            line["cpu_baseline"], ref_line = cpu_baseline_subprocess(args, chk)
+        for name, r in ref_line.get("check", {}).items():
+            tgt = line if name == args.path else line.get(name)
+            if tgt is not None:
+                tgt["exact_on_sample"] = r["exact"]
+                tgt["max_abs_error_on_sample"] = r["max_abs_error"]
+        if ours_gpu is not None:
+            line["ref_gpu"] = merge_gpu_cases(ours_gpu, ref_line.get("ref_gpu"))
+            line["nvbench"] = merge_nvbench(ours_nv, ref_line.get("nvbench"))
+    elif ours_gpu is not None:
+        line["ref_gpu"] = merge_gpu_cases(ours_gpu, None)
+        line["nvbench"] = merge_nvbench(ours_nv, None)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

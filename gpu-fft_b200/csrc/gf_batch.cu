@@ -357,9 +357,8 @@ template <typename T> __global__ void batch_tables_kernel(cx<T>* tab, int m)
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < H)
     {
-        const unsigned br = (m > 1) ? (__brev((unsigned)i) >> (33 - m)) : 0u;
         double sn, cs;
-        sincospi(2.0 * (double)br / (double)M, &sn, &cs);
+        native_root(i, m, cs, sn);
         tab[i] = mk<T>((T)cs, (T)sn);
         tab[H + i] = mk<T>((T)cs, (T)-sn);
     }

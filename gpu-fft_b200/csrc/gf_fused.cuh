@@ -26,6 +26,26 @@ template <typename T> struct FusedArgs
               // COMPLEX<T> rows, c is scaled, SINGLE only
 };
 
+// Root i (0 <= i < M/2) of the native tables of a 2^m-point transform:
+// exp(2 pi i br(i) / M), br the m-1 bit reversal, in double precision. Odd
+// entries are exactly i times their even neighbour (bit reversal makes index
+// 2j+1 the angle of 2j plus a quarter turn), and the tables store that relation
+// exactly: kernels of the native products load the even entry only and rotate
+// it. Every generator of native tables goes through this function.
+__device__ __forceinline__ void native_root(long long i, int m, double& c, double& s)
+{
+    const long long M = 1LL << m;
+    const long long ie = i & ~1LL;
+    const unsigned br = (m > 1) ? (__brev((unsigned)ie) >> (33 - m)) : 0u;
+    sincospi(2.0 * (double)br / (double)M, &s, &c);
+    if (i & 1)
+    {
+        const double t = c;
+        c = -s;
+        s = t;
+    }
+}
+
 // Contiguous pass over both operands: all forward stages of the pass on A and
 // B, the pointwise product, and all inverse stages on the product. SINGLE: the
 // pass is the whole transform (fold + twist in the load, scale + untwist +

@@ -48,20 +48,8 @@ template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < H)
     {
-        // odd entries are exactly i times their even neighbour: bit reversal
-        // makes index 2j+1 the angle of 2j plus a quarter turn, and the table
-        // stores that relation exactly (kernels of the native products may
-        // load the even entry only and rotate it)
-        const long long ie = i & ~1LL;
-        const unsigned br = (m > 1) ? (__brev((unsigned)ie) >> (33 - m)) : 0u;
         double s, c;
-        sincospi(2.0 * (double)br / (double)M, &s, &c);
-        if (i & 1)
-        {
-            const double t = c;
-            c = -s;
-            s = t;
-        }
+        native_root(i, m, c, s);
         tab[i] = mk<T>((T)c, (T)s);
         tab[H + i] = mk<T>((T)c, (T)-s);
     }

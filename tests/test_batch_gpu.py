@@ -84,6 +84,11 @@ def test_batch_4096_mixed_sizes_graph_and_autotune(gf, O, dev):
         n = 1 << np_
         ref = gf.negacyclic_mul(a[o0:o0 + len(idx) * n].view(len(idx), n), b[o0:o0 + len(idx) * n].view(len(idx), n))
         assert torch.equal(c0[o0:o0 + len(idx) * n].view(len(idx), n), ref), np_
+    # the per-class chains: about 512 requests per class, so the classes above
+    # 2^12 run the non-cluster middle pass on the plan's own tables
+    plan.set_shape(0, 1)
+    assert torch.equal(plan.execute(a, b), c0)
+    plan.set_shape(1, 1)
     # |c| < 2^47: exact against the __int128 product on sampled coefficients
     for i in rng.choice(len(n_powers), 12, replace=False):
         n = 1 << n_powers[i]
