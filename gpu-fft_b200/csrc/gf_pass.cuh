@@ -677,6 +677,34 @@ static inline int launch_pass(const PassArgs<T>& a, const Plan& p, int k, long l
             c.do_scale = a.do_scale;
             return launch_cluster_pass<T, FWD ? CLM_FWD : CLM_INV>(c, ctas, a.batch, s);
         }
+        // a whole transform of 2^10 .. 2^12 points in one pass, few rows: one
+        // cluster of 2^(L-9) CTAs per row instead of one CTA for the whole
+        // transform (or for several rows)
+        const bool in_ok = FWD ? (a.in_kind == IN_CPX || a.in_kind == IN_FOLD)
+                               : (a.in_kind == IN_CPX || a.in_kind == IN_PROD);
+        const bool out_ok = FWD ? a.out_kind == OUT_CPX : (a.out_kind == OUT_CPX || a.out_kind == OUT_UNFOLD);
+        if (p.np == 1 && L >= 10 && L == a.geo.m && in_ok && out_ok && !a.zero_pad && !a.perm &&
+            cluster_ok(a.batch))
+        {
+            ClusterArgs<T> c{};
+            c.in = static_cast<const cx<T>*>(a.in);
+            c.out = static_cast<cx<T>*>(a.out);
+            c.table = a.table;
+            c.inv_table = a.table;
+            c.scale = a.scale;
+            c.prod_off = a.prod_off;
+            c.m = a.geo.m;
+            c.neg = a.geo.neg;
+            c.prod = a.in_kind == IN_PROD;
+            c.do_scale = a.do_scale;
+            c.in_kind = a.in_kind == IN_FOLD ? CL_IN_FOLD : CL_IN_CPX;
+            c.out_kind = a.out_kind == OUT_UNFOLD ? CL_OUT_UNFOLD : CL_OUT_CPX;
+            c.rin = static_cast<const T*>(a.in);
+            c.rout = static_cast<T*>(a.out);
+            c.twist = a.twist;
+            c.untwist = a.twist;
+            return launch_cluster_pass<T, FWD ? CLM_FWD : CLM_INV>(c, a.batch, a.batch, s, L);
+        }
         return dispatch_int<1, EBITS>(L, [&]<int LL>() { return launch_pass_shape<T, FWD, LL, false>(a, ctas, s); });
     }
     if (L <= COL_MAX_L)

@@ -133,6 +133,37 @@ template <typename T, bool SINGLE> static int launch_fused(const FusedArgs<T>& a
         if (g_f64_middle_r8.load(std::memory_order_relaxed)) return launch_fused_r8(a, ctas, s);
     }
     if (!SINGLE) return launch_fused_shape<T, EBITS, false>(a, ctas, s);
+    if (a.geo.m >= 10 && cluster_ok(a.batch))
+    {
+        // few products of 2^10 .. 2^12 points: each product on one cluster of
+        // 2^(m-9) CTAs (fold or linear load, product, unfold, or the cyclic
+        // product's complex rows) instead of one CTA for whole products
+        ClusterArgs<T> c{};
+        c.table = a.roots;
+        c.inv_table = a.inv_roots;
+        c.m = a.geo.m;
+        c.scale = mk<T>(a.scale, T(0));
+        if (a.cplx)
+        {
+            c.in = reinterpret_cast<const cx<T>*>(a.a);
+            c.in2 = reinterpret_cast<const cx<T>*>(a.b);
+            c.out = reinterpret_cast<cx<T>*>(a.c);
+            c.do_scale = 1;
+            c.in_kind = CL_IN_CPX;
+            c.out_kind = CL_OUT_CPX;
+        }
+        else
+        {
+            c.rin = a.a;
+            c.rin2 = a.b;
+            c.rout = a.c;
+            c.twist = a.twist;
+            c.untwist = a.untwist;
+            c.in_kind = a.lin ? CL_IN_LIN : CL_IN_FOLD;
+            c.out_kind = CL_OUT_UNFOLD;
+        }
+        return launch_cluster_pass<T, CLM_FUSED>(c, a.batch, a.batch, s, a.geo.m);
+    }
     return dispatch_int<1, EBITS>(a.geo.m, [&]<int LL>() { return launch_fused_shape<T, LL, true>(a, ctas, s); });
 }
 

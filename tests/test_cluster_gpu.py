@@ -1,5 +1,7 @@
 """GPU tests of the cluster form of the contiguous 12-stage pass (few tiles:
-each 4096-point tile spread over 8 CTAs through distributed shared memory).
+each 4096-point tile spread over 8 CTAs through distributed shared memory),
+and of its single-pass form for whole transforms of 2^10..2^12 points (2, 4
+or 8 CTAs per row, with the FFNT fold / unfold and the linear-product load).
 It runs the engine's butterflies with the same twiddles in the same stage
 order, so every result must be bit-identical to the one-CTA-per-tile form:
 each case runs twice, with the cluster form forced on and off. Parity with
@@ -38,7 +40,8 @@ def test_limit_roundtrip(gf):
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-@pytest.mark.parametrize("n_power,batch", [(14, 1), (16, 1), (16, 3), (17, 2), (18, 1), (20, 1), (22, 1)])
+@pytest.mark.parametrize("n_power,batch", [(11, 1), (12, 2), (13, 1), (13, 64), (14, 1), (16, 1), (16, 3), (17, 2),
+                                           (18, 1), (20, 1), (22, 1)])
 def test_negacyclic_mul_cluster_identical(gf, dev, both, dtype, n_power, batch):
     g = torch.Generator().manual_seed(n_power * 11 + batch)
     n = 1 << n_power
@@ -59,7 +62,7 @@ def test_negacyclic_mul_cluster_identical(gf, dev, both, dtype, n_power, batch):
 
 
 @pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
-@pytest.mark.parametrize("n_power,batch", [(13, 1), (15, 2), (17, 1)])
+@pytest.mark.parametrize("n_power,batch", [(10, 1), (11, 3), (12, 2), (13, 1), (15, 2), (17, 1)])
 def test_cyclic_mul_cluster_identical(gf, dev, both, dtype, n_power, batch):
     g = torch.Generator().manual_seed(n_power + 5 * batch)
     M = 1 << n_power
@@ -70,7 +73,8 @@ def test_cyclic_mul_cluster_identical(gf, dev, both, dtype, n_power, batch):
 
 
 @pytest.mark.parametrize("T", [np.float64, np.float32])
-@pytest.mark.parametrize("n_power,neg", [(13, 0), (15, 0), (14, 1), (17, 1)])
+@pytest.mark.parametrize("n_power,neg", [(10, 0), (11, 0), (12, 0), (10, 1), (12, 1), (13, 0), (15, 0), (14, 1),
+                                         (17, 1)])
 def test_c2c_cluster_identical(gf, O, dev, both, T, n_power, neg):
     rng = np.random.default_rng(300 + n_power)
     M = 1 << n_power
@@ -95,7 +99,7 @@ def test_c2c_cluster_identical(gf, O, dev, both, T, n_power, neg):
     assert torch.equal(on, off)
 
 
-@pytest.mark.parametrize("n_power", [14, 16, 17])
+@pytest.mark.parametrize("n_power", [11, 12, 13, 14, 16, 17])
 def test_ffnt_dropin_cluster_identical(gf, O, dev, both, n_power):
     n = 1 << n_power
     h = n // 2
@@ -115,6 +119,18 @@ def test_ffnt_dropin_cluster_identical(gf, O, dev, both, n_power):
         return torch.cat([inout, torch.view_as_real(temp).ravel()])
 
     on, off = both(run)
+    assert torch.equal(on, off)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("n_power,batch", [(10, 1), (11, 2), (12, 1), (13, 1)])
+def test_linear_mul_cluster_identical(gf, dev, both, dtype, n_power, batch):
+    # rows of N = 2^n_power reals, product rows of 2N: one pass of 2^n_power points
+    g = torch.Generator().manual_seed(n_power * 3 + batch)
+    n = 1 << n_power
+    a = torch.randn((batch, n), generator=g).to(dtype).to(dev)
+    b = torch.randn((batch, n), generator=g).to(dtype).to(dev)
+    on, off = both(lambda: gf.linear_mul(a, b).clone())
     assert torch.equal(on, off)
 
 

@@ -7,7 +7,9 @@ layout rules (gpu-fft_b200/csrc/gf_cluster.cuh, gf_special.cu, gf_engine.cuh):
   each CTA's 512 points; DSMEM exchanges into padded buffers) must perform
   exactly the butterflies of the plain stage loop -- stage u on e-bit 11 - u
   with table[(g << u) + (e >> (12 - u))] -- for the fused, forward and inverse
-  modes, cyclic and negacyclic indexing;
+  modes, cyclic and negacyclic indexing; and so must its single-pass form for
+  2^LT-point transforms, LT = 10, 11 (2^(LT-9) CTAs; X register k = (h, lo)
+  holds e = 64 c + t + 64 2^(LT-9) lo + 512 h);
 * the special-FFT cluster pass must perform the special network's spans
   2^0..2^11 with table[2^q + (e mod 2^q)];
 * every shared-memory slot stays inside its buffer, every exchange slot is
@@ -43,11 +45,11 @@ def gs(x, y, w):
 
 
 # ---------------------------------------------------------------- the FFT pass
-def plain_pass(x, tab, g, fwd):
+def plain_pass(x, tab, g, fwd, lt=12):
     x = list(x)
-    for u in (range(12) if fwd else range(11, -1, -1)):
-        q = 11 - u
-        for e in range(4096):
+    for u in (range(lt) if fwd else range(lt - 1, -1, -1)):
+        q = lt - 1 - u
+        for e in range(1 << lt):
             if e >> q & 1:
                 continue
             w = tab[(g << u) + (e >> (q + 1))]
@@ -55,11 +57,11 @@ def plain_pass(x, tab, g, fwd):
     return x
 
 
-def cl_round(regs, p, ebase, tab, g, fwd):
+def cl_round(regs, p, ebase, tab, g, fwd, lt=12):
     for k in range(3):
         i = 2 - k if fwd else k
         q = p + i
-        u = 11 - q
+        u = lt - 1 - q
         base = (g << u) + (ebase >> (q + 1))
         w = []
         for h in range(4 >> i):
@@ -72,86 +74,120 @@ def cl_round(regs, p, ebase, tab, g, fwd):
                 arr[r], arr[r | (1 << i)] = (ct if fwd else gs)(arr[r], arr[r | (1 << i)], w[r >> (i + 1)])
 
 
-def transpose(state, bufs, ya, yb, na):
-    for c in range(CL):
+def cl_xround(regs, tab, g, fwd, lt):
+    """The cross-CTA stages: e-bits 9..lt-1 on register bits lob..2."""
+    lc = lt - 9
+    lob = 3 - lc
+    for k in range(lc):
+        i = lc - 1 - k if fwd else k
+        u = lt - 1 - (9 + i)
+        w = []
+        for h in range((1 << lc) >> (i + 1)):
+            assert 0 <= (g << u) + h < len(tab)
+            w.append(tab[(g << u) + h])
+        for r in range(8):
+            if r >> (lob + i) & 1:
+                continue
+            for arr in regs:
+                b = r | (1 << (lob + i))
+                arr[r], arr[b] = (ct if fwd else gs)(arr[r], arr[b], w[(r >> lob) >> (i + 1)])
+
+
+def transpose(state, bufs, ya, yb, na, cl=CL):
+    for c in range(cl):
         for t in range(TH):
             for a in range(na):
                 for r in range(8):
                     slot = cpad(ypos(ya, t, r))
                     assert slot < SMEM
                     bufs[c][a][slot] = state[c, t][a][r]
-    for c in range(CL):
+    for c in range(cl):
         for t in range(TH):
             state[c, t] = [[bufs[c][a][cpad(ypos(yb, t, r))] for r in range(8)] for a in range(na)]
 
 
-def cluster_pass(mode, ops, tab, itab, g):
+def cluster_pass(mode, ops, tab, itab, g, lt=12):
     na = 2 if mode == "fused" else 1
-    ybuf = [[[None] * SMEM for _ in range(na)] for _ in range(CL)]
-    xbuf = [[[None] * SMEM] for _ in range(CL)]
+    lc = lt - 9
+    cl, lob = 1 << lc, 3 - lc
+
+    def xl(c, t, k):  # local point of X register k (in CTA k >> lob)
+        return 64 * c + t + 64 * cl * (k & ((1 << lob) - 1))
+
+    def xe(c, t, k):
+        return xl(c, t, k) + 512 * (k >> lob)
+
+    ybuf = [[[None] * SMEM for _ in range(na)] for _ in range(cl)]
+    xbuf = [[[None] * SMEM] for _ in range(cl)]
     st = {}
-    out = [None] * 4096
+    out = [None] * (1 << lt)
     if mode == "inv":
-        for c in range(CL):
+        for c in range(cl):
             for t in range(TH):
                 st[c, t] = [[ops[0][512 * c + ypos(1, t, r)] for r in range(8)]]
-        transpose(st, ybuf, 1, 3, 1)
+        transpose(st, ybuf, 1, 3, 1, cl)
     else:
-        for c in range(CL):
+        seen = set()
+        for c in range(cl):
             for t in range(TH):
-                ex = 64 * c + t
-                st[c, t] = [[ops[a][ex + 512 * k] for k in range(8)] for a in range(na)]
-                cl_round(st[c, t], 9, ex, tab, g, True)
-        for c in range(CL):  # X -> Y1: register k to CTA k at slot ex
+                for k in range(8):
+                    assert xe(c, t, k) not in seen
+                    seen.add(xe(c, t, k))
+                st[c, t] = [[ops[a][xe(c, t, k)] for k in range(8)] for a in range(na)]
+                cl_xround(st[c, t], tab, g, True, lt)
+        assert seen == set(range(1 << lt))
+        for c in range(cl):  # X -> Y1: register k to CTA k >> lob at its local point
             for t in range(TH):
                 for k in range(8):
                     for a in range(na):
-                        slot = cpad(64 * c + t)
-                        assert ybuf[k][a][slot] is None
-                        ybuf[k][a][slot] = st[c, t][a][k]
-        for c in range(CL):
+                        slot = cpad(xl(c, t, k))
+                        assert slot < SMEM and ybuf[k >> lob][a][slot] is None
+                        ybuf[k >> lob][a][slot] = st[c, t][a][k]
+        for c in range(cl):
             for t in range(TH):
                 st[c, t] = [[ybuf[c][a][cpad(ypos(1, t, r))] for r in range(8)] for a in range(na)]
-                cl_round(st[c, t], 6, 512 * c + ypos(1, t, 0), tab, g, True)
+                cl_round(st[c, t], 6, 512 * c + ypos(1, t, 0), tab, g, True, lt)
         for ya, yb, p in ((1, 2, 3), (2, 3, 0)):
-            transpose(st, ybuf, ya, yb, na)
-            for c in range(CL):
+            transpose(st, ybuf, ya, yb, na, cl)
+            for c in range(cl):
                 for t in range(TH):
-                    cl_round(st[c, t], p, 512 * c + ypos(yb, t, 0), tab, g, True)
+                    cl_round(st[c, t], p, 512 * c + ypos(yb, t, 0), tab, g, True, lt)
         if mode == "fwd":
-            transpose(st, ybuf, 3, 1, 1)
-            for c in range(CL):
+            transpose(st, ybuf, 3, 1, 1, cl)
+            for c in range(cl):
                 for t in range(TH):
                     for r in range(8):
                         e = 512 * c + ypos(1, t, r)
                         assert out[e] is None
                         out[e] = st[c, t][0][r]
             return out
-        for c in range(CL):
+        for c in range(cl):
             for t in range(TH):
                 st[c, t] = [[st[c, t][0][r] * st[c, t][1][r] for r in range(8)]]
-    for c in range(CL):
+    for c in range(cl):
         for t in range(TH):
-            cl_round(st[c, t], 0, 512 * c + ypos(3, t, 0), itab, g, False)
+            cl_round(st[c, t], 0, 512 * c + ypos(3, t, 0), itab, g, False, lt)
     for ya, yb, p in ((3, 2, 3), (2, 1, 6)):
-        transpose(st, ybuf, ya, yb, 1)
-        for c in range(CL):
+        transpose(st, ybuf, ya, yb, 1, cl)
+        for c in range(cl):
             for t in range(TH):
-                cl_round(st[c, t], p, 512 * c + ypos(yb, t, 0), itab, g, False)
-    for c in range(CL):  # Y1 -> X: point 512 c + t + 64 r to CTA r, slot 64 c + t
+                cl_round(st[c, t], p, 512 * c + ypos(yb, t, 0), itab, g, False, lt)
+    for c in range(cl):  # Y1 -> X: point 512 c + t + 64 r to CTA r & (cl-1), register (c << lob) | (r >> lc)
         for t in range(TH):
             for r in range(8):
-                slot = cpad(64 * c + t)
-                assert xbuf[r][0][slot] is None
-                xbuf[r][0][slot] = st[c, t][0][r]
-    for c in range(CL):
+                k = (c << lob) | (r >> lc)
+                dst = r & (cl - 1)
+                assert xe(dst, t, k) == 512 * c + t + 64 * r
+                slot = cpad(64 * k + t)
+                assert slot < SMEM and xbuf[dst][0][slot] is None
+                xbuf[dst][0][slot] = st[c, t][0][r]
+    for c in range(cl):
         for t in range(TH):
-            ex = 64 * c + t
             z = [[xbuf[c][0][cpad(64 * k + t)] for k in range(8)]]
-            cl_round(z, 9, ex, itab, g, False)
+            cl_xround(z, itab, g, False, lt)
             for k in range(8):
-                assert out[ex + 512 * k] is None
-                out[ex + 512 * k] = z[0][k]
+                assert out[xe(c, t, k)] is None
+                out[xe(c, t, k)] = z[0][k]
     return out
 
 
@@ -172,6 +208,22 @@ def test_cluster_pass_schedule(m, tile, neg):
     assert cluster_pass("inv", [a], itab, itab, g) == plain_pass(a, itab, g, False)
     prod = [x * y for x, y in zip(fa, fb)]
     assert cluster_pass("fused", [a, b], tab, itab, g) == plain_pass(prod, itab, g, False)
+
+
+@pytest.mark.parametrize("lt,neg", [(10, 0), (11, 0), (12, 0), (11, 1), (10, 1)])
+def test_single_pass_cluster_schedule(lt, neg):
+    # a whole transform of 2^lt points (one tile, group 0 at stage 0)
+    rng = np.random.default_rng(90 + lt + neg)
+    size = (1 << (lt + 1)) if neg else (1 << (lt - 1))
+    tab, itab = cvec(rng, size), cvec(rng, size)
+    g = 1 if neg else 0
+    n = 1 << lt
+    a, b = cvec(rng, n), cvec(rng, n)
+    fa, fb = plain_pass(a, tab, g, True, lt), plain_pass(b, tab, g, True, lt)
+    assert cluster_pass("fwd", [a], tab, itab, g, lt) == fa
+    assert cluster_pass("inv", [a], itab, itab, g, lt) == plain_pass(a, itab, g, False, lt)
+    prod = [x * y for x, y in zip(fa, fb)]
+    assert cluster_pass("fused", [a, b], tab, itab, g, lt) == plain_pass(prod, itab, g, False, lt)
 
 
 # ------------------------------------------------------------ the special FFT

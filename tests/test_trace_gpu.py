@@ -23,7 +23,9 @@ def test_trace_records_the_fused_chain(gf, dev):
     finally:
         gf.trace_enable(False)
     rows = {r["kernel"]: r for r in gf.trace_collect()}
-    fused = rows["fused_kernel<f64,L12,middle>"]
+    # the FP64 middle pass: 512 threads x 8 points (the default) or 256 x 16
+    middle = "fused_r8_kernel<f64,L12,middle>" if gf.set_f64_middle(-1) else "fused_kernel<f64,L12,middle>"
+    fused = rows[middle]
     first = [r for k, r in rows.items() if k.startswith("col_pass<f64,fwd,L3")]
     last = [r for k, r in rows.items() if k.startswith("col_pass<f64,inv,L3")]
     assert len(first) == 1 and len(last) == 1
