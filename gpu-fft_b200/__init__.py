@@ -144,6 +144,8 @@ def lib() -> ctypes.CDLL:
         L.gpufft_version.restype = i
         L.gpufft_set_cluster_tiles.argtypes = [i]
         L.gpufft_set_cluster_tiles.restype = i
+        L.gpufft_set_programmatic_launch.argtypes = [i]
+        L.gpufft_set_programmatic_launch.restype = i
         L.gpufft_batch_plan_set_barrier.argtypes = [vp, ctypes.c_uint, ctypes.c_uint]
         L.gpufft_set_f64_middle.argtypes = [i]
         L.gpufft_set_f64_middle.restype = i
@@ -427,6 +429,13 @@ def set_cluster_tiles(max_tiles: int) -> int:
     as 8-CTA clusters (small batches); 0 disables, a negative value queries.
     Results are bit-identical either way. Returns the previous limit."""
     return int(lib().gpufft_set_cluster_tiles(int(max_tiles)))
+
+
+def set_programmatic_launch(on: int) -> int:
+    """Chain kernels launched with programmatic stream serialization (1, the
+    default) or in plain stream order (0); identical results. A negative value
+    queries. Returns the previous setting."""
+    return int(lib().gpufft_set_programmatic_launch(int(on)))
 
 
 def trace_enable(on: bool = True) -> None:

@@ -202,6 +202,7 @@ __device__ __forceinline__ void cl_transpose(cx<T> (&x)[NA][8], cx<T> (*buf)[CL_
 template <typename T, int MODE, int LT>
 __global__ void __cluster_dims__(1 << (LT - 9), 1, 1) __launch_bounds__(CL_THREADS) cluster_pass_kernel(const ClusterArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int NA = MODE == CLM_FUSED ? 2 : 1;
     constexpr int LC = LT - 9, CT = 1 << LC, LOB = 3 - LC;
     __shared__ __align__(16) cx<T> ybuf[NA][CL_SMEM];
@@ -390,13 +391,9 @@ static inline int launch_cluster_pass(const ClusterArgs<T>& a, long long tiles, 
     const double nin = MODE == CLM_FUSED ? 2.0 : ((MODE == CLM_INV && a.prod) ? 2.0 : 1.0);
     GF_TRACE(tr, pts * (nin * (MODE == CLM_INV ? cb : in_b) + cb), s, "cluster_pass<%s,%s,L%d>",
              sizeof(T) == 4 ? "f32" : "f64", MODE == CLM_FWD ? "fwd" : (MODE == CLM_INV ? "inv" : "fused"), lt);
-    if (lt == 12)
-        cluster_pass_kernel<T, MODE, 12><<<dim3((unsigned)ctas), dim3(CL_THREADS), 0, s>>>(a);
-    else if (lt == 11)
-        cluster_pass_kernel<T, MODE, 11><<<dim3((unsigned)ctas), dim3(CL_THREADS), 0, s>>>(a);
-    else
-        cluster_pass_kernel<T, MODE, 10><<<dim3((unsigned)ctas), dim3(CL_THREADS), 0, s>>>(a);
-    return check_launch();
+    if (lt == 12) return launch_k(cluster_pass_kernel<T, MODE, 12>, dim3((unsigned)ctas), dim3(CL_THREADS), 0, s, a);
+    if (lt == 11) return launch_k(cluster_pass_kernel<T, MODE, 11>, dim3((unsigned)ctas), dim3(CL_THREADS), 0, s, a);
+    return launch_k(cluster_pass_kernel<T, MODE, 10>, dim3((unsigned)ctas), dim3(CL_THREADS), 0, s, a);
 }
 
 } // namespace gfb

@@ -6,7 +6,9 @@
 // with the multiply-add rounding fixed explicitly (see cmul).
 #pragma once
 
+#include <atomic>
 #include <cstdio>
+#include <utility>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -82,6 +84,21 @@ template <typename T> __device__ __forceinline__ T ldg_s(const T* p) { return __
 template <typename V> __device__ __forceinline__ V ld_stream(const V* p) { return __ldcs(p); }
 template <typename V> __device__ __forceinline__ void st_stream(V* p, V v) { __stcs(p, v); }
 
+// Programmatic dependent launch. The chain kernels are launched with the
+// programmatic-serialization attribute (launch_k below), so a kernel's CTAs
+// may be scheduled while the previous kernel in the stream is still running.
+// Each such kernel calls pdl_begin() before its first global-memory access:
+// griddepcontrol.wait returns once every prerequisite grid has completed and
+// its writes are visible (at once when the kernel was launched without the
+// attribute); launch_dependents then lets the next kernel's CTAs be scheduled
+// early in turn. Waiting first keeps at most one grid waiting behind a
+// running one.
+__device__ __forceinline__ void pdl_begin()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 } // namespace gfb
 
 // Host-side status plumbing shared by every entry point.
@@ -89,6 +106,28 @@ namespace gfb
 {
 int set_cuda_error(cudaError_t e);
 int check_launch();
+
+// Launches of the chain kernels (each starts with pdl_begin): with the
+// programmatic-serialization attribute while g_pdl is set
+// (gpufft_set_programmatic_launch), plain stream order otherwise.
+extern std::atomic<int> g_pdl;
+template <typename... P, typename... A>
+inline int launch_k(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_pdl.load(std::memory_order_relaxed) ? 1 : 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    return check_launch();
+}
 
 // Per-kernel device-time tracing (gpufft_trace_enable / gpufft_trace_collect).
 // While tracing is on, every kernel launch of the product paths is bracketed

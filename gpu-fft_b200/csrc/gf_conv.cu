@@ -41,6 +41,7 @@ struct VjpArgs
 
 template <int L, bool SINGLE> __global__ void __launch_bounds__(NTHR, 1) vjp_kernel(const VjpArgs a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
     using S = Sched<0, L>;
@@ -122,8 +123,7 @@ template <int L, bool SINGLE> static int launch_vjp_shape(const VjpArgs& a, long
     // three spectra (G, A, B) in, two gradients out, per point of the half-length transform
     GF_TRACE(tr, (double)a.batch * (double)(1LL << a.geo.m) * 5 * sizeof(cx<float>), s, "vjp_kernel<L%d,%s>", L,
              SINGLE ? "single" : "middle");
-    vjp_kernel<L, SINGLE><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
-    return check_launch();
+    return launch_k(vjp_kernel<L, SINGLE>, dim3((unsigned)ctas), dim3(NTHR), smem, s, a);
 }
 
 static long long vjp_wave(int m, long long batch)

@@ -111,6 +111,7 @@ constexpr size_t smem_bytes(size_t cxb) { return 2 * (size_t)BUF * cxb; }
 // inverse stages overwrite A's tile.
 template <typename T> __global__ void __launch_bounds__(r8::THREADS, 1) fused_r8_kernel(const FusedArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     using namespace r8;
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);

@@ -414,6 +414,7 @@ template <typename T> constexpr int pass_min_blocks() { return sizeof(T) == 4 ? 
 template <typename T, bool FWD, int L, bool STRIDED, bool PERM = false>
 __global__ void __launch_bounds__(NTHR, pass_min_blocks<T>()) pass_kernel(const PassArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     extern __shared__ __align__(16) unsigned char smraw[];
     pass_body<T, FWD, L, STRIDED, PERM>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
 }
@@ -538,6 +539,7 @@ __device__ __forceinline__ void col_pass_body(const PassArgs<T>& a, long long id
 template <typename T, bool FWD, int L, int IK, int OK>
 __global__ void __launch_bounds__(COL_THREADS) col_pass_kernel(const PassArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     col_pass_body<T, FWD, L, IK, OK>(a, (long long)blockIdx.x * COL_THREADS + threadIdx.x);
 }
 
@@ -552,8 +554,7 @@ static inline int launch_col_pass(const PassArgs<T>& a, cudaStream_t s)
     auto go = [&](auto kern) {
         GF_TRACE(tr, pass_alg_bytes(a), s, "col_pass<%s,%s,L%d,in%d,out%d>", sizeof(T) == 4 ? "f32" : "f64",
                  kind_name(FWD), L, a.in_kind, a.out_kind);
-        kern<<<blocks, COL_THREADS, 0, s>>>(a);
-        return check_launch();
+        return launch_k(kern, blocks, COL_THREADS, 0, s, a);
     };
     if constexpr (FWD)
     {
@@ -646,8 +647,7 @@ static inline int launch_pass_shape(const PassArgs<T>& a, long long ctas, cudaSt
     if (st) return st;
     GF_TRACE(tr, pass_alg_bytes(a), s, "pass_kernel<%s,%s,L%d,%s>", sizeof(T) == 4 ? "f32" : "f64",
              kind_name(FWD), L, STRIDED ? "strided" : "contiguous");
-    pass_kernel<T, FWD, L, STRIDED, PERM><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
-    return check_launch();
+    return launch_k(pass_kernel<T, FWD, L, STRIDED, PERM>, dim3((unsigned)ctas), dim3(NTHR), smem, s, a);
 }
 
 // Launch pass k of plan p (the pass's L selects the compiled shape).

@@ -74,6 +74,7 @@ template <typename T> __global__ void ffnt_tables_kernel(cx<T>* tab, int m)
 template <typename T, int L, bool SINGLE>
 __global__ void __launch_bounds__(NTHR, sizeof(T) == 4 ? 2 : 1) fused_kernel(const FusedArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     extern __shared__ __align__(16) unsigned char smraw[];
     fused_body<T, L, SINGLE>(a, blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
 }
@@ -90,8 +91,7 @@ static int launch_fused_shape(const FusedArgs<T>& a, long long ctas, cudaStream_
     const double M = (double)(1LL << a.geo.m);
     GF_TRACE(tr, (double)a.batch * M * 6.0 * sizeof(T), s, "fused_kernel<%s,L%d,%s>", sizeof(T) == 4 ? "f32" : "f64",
              L, SINGLE ? "single" : "middle");
-    fused_kernel<T, L, SINGLE><<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
-    return check_launch();
+    return launch_k(fused_kernel<T, L, SINGLE>, dim3((unsigned)ctas), dim3(NTHR), smem, s, a);
 }
 
 // The FP64 middle pass runs on 512 threads x 8 points per operand
@@ -107,8 +107,7 @@ static int launch_fused_r8(const FusedArgs<double>& a, long long ctas, cudaStrea
     if (st) return st;
     const double M = (double)(1LL << a.geo.m);
     GF_TRACE(tr, (double)a.batch * M * 6.0 * sizeof(double), s, "fused_r8_kernel<f64,L12,middle>");
-    fused_r8_kernel<double><<<dim3((unsigned)ctas), dim3(r8::THREADS), smem, s>>>(a);
-    return check_launch();
+    return launch_k(fused_r8_kernel<double>, dim3((unsigned)ctas), dim3(r8::THREADS), smem, s, a);
 }
 
 template <typename T, bool SINGLE> static int launch_fused(const FusedArgs<T>& a, long long ctas, cudaStream_t s)

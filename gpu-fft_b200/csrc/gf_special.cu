@@ -84,6 +84,7 @@ __device__ __forceinline__ void special_network(cx<T> (&x)[1 << L], const cx<T> 
 template <typename T, int L, bool FWD>
 __global__ void __launch_bounds__(SPECIAL_THREADS) special_col_kernel(const SpecialArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L;
     const long long idx = (long long)blockIdx.x * SPECIAL_THREADS + threadIdx.x;
     const int m = a.m, p0 = a.p0;
@@ -109,6 +110,7 @@ __global__ void __launch_bounds__(SPECIAL_THREADS) special_col_kernel(const Spec
 template <typename T, int L, bool FWD>
 __global__ void __launch_bounds__(SPECIAL_THREADS) special_first_kernel(const SpecialArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L;
     constexpr int RUN = SPECIAL_THREADS * R;
     __shared__ cx<T> sm[RUN + RUN / 16];
@@ -186,6 +188,7 @@ __device__ __forceinline__ void special_cl_round(cx<T> (&x)[1][8], int ebase, co
 template <typename T, bool FWD>
 __global__ void __cluster_dims__(CL_CTAS, 1, 1) __launch_bounds__(CL_THREADS) special_cluster_kernel(const SpecialArgs<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     __shared__ __align__(16) cx<T> ybuf[1][CL_SMEM];
     __shared__ __align__(16) cx<T> xbuf[1][CL_SMEM];
     cgx::cluster_group cluster = cgx::this_cluster();
@@ -258,8 +261,7 @@ template <typename T, bool FWD> static int launch_special_cluster(const SpecialA
     const long long tiles = (a.batch << a.m) >> EBITS;
     GF_TRACE(tr, (double)(a.batch << a.m) * 2 * sizeof(cx<T>), s, "special_cluster<%s,%s>",
              sizeof(T) == 4 ? "f32" : "f64", FWD ? "fwd" : "inv");
-    special_cluster_kernel<T, FWD><<<(unsigned)(tiles * CL_CTAS), CL_THREADS, 0, s>>>(a);
-    return check_launch();
+    return launch_k(special_cluster_kernel<T, FWD>, (unsigned)(tiles * CL_CTAS), CL_THREADS, 0, s, a);
 }
 
 template <typename T, bool FWD> static int launch_special_pass(const SpecialArgs<T>& a, int L, cudaStream_t s)
@@ -271,15 +273,13 @@ template <typename T, bool FWD> static int launch_special_pass(const SpecialArgs
         if (a.p0 == 0)
         {
             constexpr long long RUN = (long long)SPECIAL_THREADS << LL;
-            special_first_kernel<T, LL, FWD><<<(unsigned)((points + RUN - 1) / RUN), SPECIAL_THREADS, 0, s>>>(a);
+            return launch_k(special_first_kernel<T, LL, FWD>, dim3((unsigned)((points + RUN - 1) / RUN)),
+                            dim3(SPECIAL_THREADS), 0, s, a);
         }
-        else
-        {
-            const long long threads = points >> LL;
-            special_col_kernel<T, LL, FWD>
-                <<<(unsigned)((threads + SPECIAL_THREADS - 1) / SPECIAL_THREADS), SPECIAL_THREADS, 0, s>>>(a);
-        }
-        return check_launch();
+        const long long threads = points >> LL;
+        return launch_k(special_col_kernel<T, LL, FWD>,
+                        dim3((unsigned)((threads + SPECIAL_THREADS - 1) / SPECIAL_THREADS)), dim3(SPECIAL_THREADS), 0,
+                        s, a);
     });
 }
 

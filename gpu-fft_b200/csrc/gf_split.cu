@@ -228,8 +228,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                     GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * sizeof(cx<T>)), s,
                              "split_fwd0_col2<f32,L%d,k%d>", L0, k);
                     st = dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
-                        split_fwd0_col2<SPLIT_COL_MAX, KK><<<blocks, SPLIT_COL2_THREADS, 0, s>>>(A);
-                        return check_launch();
+                        return launch_k(split_fwd0_col2<SPLIT_COL_MAX, KK>, blocks, SPLIT_COL2_THREADS, 0, s, A);
                     });
                 }
                 else
@@ -240,8 +239,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                              "split_fwd0_col<f32,L%d,k%d>", L0, k);
                     st = dispatch_int<1, SPLIT_COL_MAX - 1>(L0, [&]<int LL>() {
                         return dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
-                            split_fwd0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
-                            return check_launch();
+                            return launch_k(split_fwd0_col<T, LL, KK>, blocks, SPLIT_COL_THREADS, 0, s, A);
                         });
                     });
                 }
@@ -255,8 +253,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                     GF_TRACE(tr, (double)wv * M * ((2 * k - 1) * sizeof(cx<T>) + 2 * 8), s,
                              "split_inv0_col2<f32,L%d,k%d>", L0, k);
                     st = dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
-                        split_inv0_col2<SPLIT_COL_MAX, KK><<<blocks, SPLIT_COL2_THREADS, 0, s>>>(A);
-                        return check_launch();
+                        return launch_k(split_inv0_col2<SPLIT_COL_MAX, KK>, blocks, SPLIT_COL2_THREADS, 0, s, A);
                     });
                 }
                 else
@@ -267,8 +264,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                              "split_inv0_col<f32,L%d,k%d>", L0, k);
                     st = dispatch_int<1, SPLIT_COL_MAX - 1>(L0, [&]<int LL>() {
                         return dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
-                            split_inv0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
-                            return check_launch();
+                            return launch_k(split_inv0_col<T, LL, KK>, blocks, SPLIT_COL_THREADS, 0, s, A);
                         });
                     });
                 }
@@ -293,8 +289,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                      F32 ? "f32" : "f64", L0, k);
             st = dispatch_int<0, SPLIT_COL_MAX>(L0, [&]<int LL>() {
                 return dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
-                    split_fwd0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
-                    return check_launch();
+                    return launch_k(split_fwd0_col<T, LL, KK>, blocks, SPLIT_COL_THREADS, 0, s, A);
                 });
             });
         }
@@ -330,8 +325,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                 GF_TRACE(tr, (double)pts * sizeof(cx<T>) * (4 * k - 1), s, "split_groups<%s,k%d>",
                          F32 ? "f32" : "f64", k);
                 st = dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
-                    split_groups<T, KK><<<(unsigned)((pts + 255) / 256), 256, 0, s>>>(A);
-                    return check_launch();
+                    return launch_k(split_groups<T, KK>, (unsigned)((pts + 255) / 256), 256, 0, s, A);
                 });
             }
             if (st) return st;
@@ -359,8 +353,7 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                      F32 ? "f32" : "f64", L0, k);
             st = dispatch_int<0, SPLIT_COL_MAX>(L0, [&]<int LL>() {
                 return dispatch_int<1, SPLIT_MAX_LIMBS>(k, [&]<int KK>() {
-                    split_inv0_col<T, LL, KK><<<blocks, SPLIT_COL_THREADS, 0, s>>>(A);
-                    return check_launch();
+                    return launch_k(split_inv0_col<T, LL, KK>, blocks, SPLIT_COL_THREADS, 0, s, A);
                 });
             });
         }

@@ -126,6 +126,7 @@ template <typename T> __device__ __forceinline__ long long uu_term(const SplitAr
 // --------------------------------------------------------------------------
 template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const SplitArgs a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
     constexpr int QOFF = EBITS - L;
@@ -177,6 +178,7 @@ template <int L> __global__ void __launch_bounds__(NTHR, 2) split_fwd0(const Spl
 // --------------------------------------------------------------------------
 template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) split_mid(const SplitArgs a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
     using S = Sched<0, L>;
@@ -332,6 +334,7 @@ template <int L, bool SINGLE, int K> __global__ void __launch_bounds__(NTHR, 2) 
 // --------------------------------------------------------------------------
 template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitArgs a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<float>* sm = reinterpret_cast<cx<float>*>(smraw);
     constexpr int QOFF = EBITS - L;
@@ -405,6 +408,7 @@ constexpr int SPLIT_COL_THREADS = 128;
 template <typename T, int L0, int K>
 __global__ void __launch_bounds__(SPLIT_COL_THREADS) split_fwd0_col(const SplitArgsT<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L0;
     const int m = a.geo.m;
     const long long M = 1LL << m, C = M >> L0;
@@ -486,6 +490,7 @@ __device__ __forceinline__ cx<float> shfl16(cx<float> v)
 
 template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5) split_fwd0_col2(const SplitArgs a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L0, H = R / 2;
     const int m = a.geo.m;
     const long long M = 1LL << m, C = M >> L0;
@@ -562,6 +567,7 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5
 
 template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4) split_inv0_col2(const SplitArgs a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L0, H = R / 2;
     const int m = a.geo.m;
     const long long M = 1LL << m, C = M >> L0;
@@ -661,6 +667,7 @@ template <typename T, int L0> constexpr int inv0_col_min_blocks() { return (size
 template <typename T, int L0, int K>
 __global__ void __launch_bounds__(SPLIT_COL_THREADS, inv0_col_min_blocks<T, L0>()) split_inv0_col(const SplitArgsT<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L0;
     const int m = a.geo.m;
     const long long M = 1LL << m, C = M >> L0;
@@ -754,6 +761,7 @@ constexpr int SPLIT_SINGLE_MAX_LIMBS = 6; // limb counts compiled for rings N <=
 // loads of a point are independent and coalesced across the warp.
 template <typename T, int K> __global__ void __launch_bounds__(256) split_groups(const SplitArgsT<T> a)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     const long long M = 1LL << a.geo.m;
     const long long n = a.W * M;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -798,8 +806,7 @@ template <typename K> static int launch_split(K* kern, int* done, const SplitArg
     // the spectra of the chain's other side (upper estimate)
     const double M = (double)(1LL << a.geo.m);
     GF_TRACE(tr, (double)a.W * M * (2 * 2 * 4 + 2 * 8 + (4 * a.k - 1) * 8), s, "split_tiled<k%d>", a.k);
-    kern<<<dim3((unsigned)ctas), dim3(NTHR), smem, s>>>(a);
-    return check_launch();
+    return launch_k(kern, dim3((unsigned)ctas), dim3(NTHR), smem, s, a);
 }
 
 template <int L, bool SINGLE, int K> static int launch_mid_k(const SplitArgs& a, long long ctas, cudaStream_t s)

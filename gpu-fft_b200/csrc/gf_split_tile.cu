@@ -13,8 +13,7 @@ template <int K> static int launch_tile_k(const SplitArgs& a, long long tiles, c
     const long long grid = tiles < (long long)sm_count() ? tiles : (long long)sm_count();
     // 2k limb tiles in, 2k-1 group tiles out
     GF_TRACE(tr, (double)tiles * stile::P * sizeof(float2) * (4 * K - 1), s, "split_tile<k%d>", K);
-    split_tile_kernel<K><<<dim3((unsigned)grid), dim3(stile::NTT), smem, s>>>(a, tiles);
-    return check_launch();
+    return launch_k(split_tile_kernel<K>, dim3((unsigned)grid), dim3(stile::NTT), smem, s, a, tiles);
 }
 
 int launch_split_tile(int k, const SplitArgs& a, long long tiles, cudaStream_t s)

@@ -271,6 +271,7 @@ static __device__ unsigned g_split_wait_timeouts;
 template <int K>
 __global__ void __launch_bounds__(stile::NTT, 1) split_tile_kernel(const SplitArgs a, long long tiles)
 {
+    pdl_begin(); // before any global-memory access (programmatic launch)
     using namespace stile;
     constexpr int NS = 2 * K;     // slots: limbs of A then B
     constexpr int NG = 2 * K - 1; // limb groups

@@ -20,6 +20,8 @@ namespace gfb
 // Contiguous 12-stage passes over at most this many 4096-point tiles run as
 // thread-block clusters (gf_cluster.cuh); 0 disables them.
 std::atomic<int> g_cluster_max_tiles{64};
+// Chain kernels launched with programmatic stream serialization (gf_common.cuh).
+std::atomic<int> g_pdl{1};
 int set_cuda_error(cudaError_t e)
 {
     g_last_cuda_error = (int)e;
@@ -191,6 +193,12 @@ extern "C" const char* gpufft_status_string(int status)
 }
 
 extern "C" int gpufft_version(void) { return 100; }
+
+extern "C" int gpufft_set_programmatic_launch(int on)
+{
+    if (on < 0) return gfb::g_pdl.load(std::memory_order_relaxed);
+    return gfb::g_pdl.exchange(on ? 1 : 0, std::memory_order_relaxed);
+}
 
 extern "C" int gpufft_set_cluster_tiles(int max_tiles)
 {

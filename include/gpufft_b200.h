@@ -71,6 +71,16 @@ int gpufft_trace_collect(int max_rows, char* names, int name_len, double* total_
  * setting: calls on other threads see either the old or the new limit). */
 int gpufft_set_cluster_tiles(int max_tiles);
 
+/* The kernels of the transform and product chains are launched with CUDA's
+ * programmatic stream serialization (programmatic dependent launch): a
+ * kernel's CTAs may be scheduled while the previous kernel in the stream
+ * runs, and each waits (griddepcontrol.wait) for that kernel to complete
+ * before touching memory, which hides most of the launch gap between the
+ * short kernels of small batches. Results are identical either way; on = 0
+ * launches in plain stream order. A negative value only queries. Returns the
+ * previous setting (default 1). Process-wide (atomic). */
+int gpufft_set_programmatic_launch(int on);
+
 /* The middle pass of the two-pass FP64 products (the last 12 forward stages of
  * both operands, their product, the first 12 inverse stages of each 4096-point
  * tile) runs on 512 threads of 8 points per operand (r8 = 1, the default) or
