@@ -196,11 +196,15 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         A.group = A.spec + (size_t)(2 * k) * wv * M;
         if constexpr (F32)
         {
-            if (m <= EBITS)
+            const long long ctas = (wv * M + ECTA - 1) / ECTA;
+            // one kernel (a CTA runs every limb and group transform of its
+            // products in turn) once it fills the SMs; fewer products take the
+            // chain below, whose passes spread those transforms over CTAs and
+            // clusters
+            if (m <= EBITS && (m < 10 || ctas >= sm_count()))
             {
                 A.geo = PassGeo{};
                 A.geo.m = m;
-                const long long ctas = (wv * M + ECTA - 1) / ECTA;
                 if (k > SPLIT_SINGLE_MAX_LIMBS) return GPUFFT_ERROR_INVALID_VALUE;
                 int st = (m <= 6)   ? launch_split_single_lo(m, A, ctas, s)
                          : (m <= 9) ? launch_split_single_mid(m, A, ctas, s)
@@ -272,8 +276,9 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                 continue;
             }
         }
-        // rings with one pass (FP64 only here) run a zero-stage column form
-        // (digits, fold, twist) around that single contiguous pass
+        // rings with one pass (FP64, and FP32 batches too small to fill the
+        // SMs) run a zero-stage column form (digits, fold, twist) around that
+        // single contiguous pass
         const int L0 = p.np == 1 ? 0 : p.L[0];
         const int kc = p.np == 1 ? 0 : 1; // the contiguous pass
         // 1. limb extraction + first forward pass (strided), all 2k limbs of a column block

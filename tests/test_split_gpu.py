@@ -19,10 +19,12 @@ def exact_rows(O, a, b, idx=None):
 
 
 @pytest.mark.parametrize("n_power,batch,lo,hi", [
-    (2, 7, 0, 1 << 24), (5, 5, -(1 << 15), 1 << 15), (10, 9, 0, 1 << 24), (12, 3, -(1 << 20), 1 << 20),
-    (13, 3, 0, 1 << 24), (14, 2, -(1 << 15), 1 << 15), (15, 2, 0, 1 << 24), (16, 2, 0, 1 << 24),
-    (17, 1, -(1 << 15), 1 << 15)])
+    (2, 7, 0, 1 << 24), (5, 5, -(1 << 15), 1 << 15), (10, 9, 0, 1 << 24), (11, 1, -(1 << 15), 1 << 15),
+    (12, 3, -(1 << 20), 1 << 20), (13, 3, 0, 1 << 24), (13, 200, 0, 1 << 24), (14, 2, -(1 << 15), 1 << 15),
+    (15, 2, 0, 1 << 24), (16, 2, 0, 1 << 24), (17, 1, -(1 << 15), 1 << 15)])
 def test_split_exact(gf, O, dev, n_power, batch, lo, hi):
+    # rings of at most 8192 run as one kernel when the batch fills the SMs
+    # (13, 200) and as the pass chain otherwise
     rng = np.random.default_rng(4000 + n_power)
     n = 1 << n_power
     a = rng.integers(lo, hi, (batch, n)).astype(np.int32)
@@ -31,7 +33,7 @@ def test_split_exact(gf, O, dev, n_power, batch, lo, hi):
     got = c.cpu().numpy()
     e = float(err.item())
     assert e < 0.5, e
-    if n_power <= 14:
+    if n_power <= 14 and batch <= 9:
         assert np.array_equal(got, exact_rows(O, a, b))
     else:  # 512 random coefficients per product against the exact O(N) formula
         idx = np.sort(rng.choice(n, 512, replace=False)).astype(np.int32)
