@@ -15,6 +15,14 @@ events on the launching stream, warm-up first; the inputs (2 x 256 x 2^16
 doubles = 256 MiB) exceed the 126 MB L2, so no flush is needed between steps.
 Multi-GPU runs (torchrun) shard the batch per rank with no collective on the
 data path (weak scaling) and report the max time over ranks.
+
+At N = 1 the line also carries: `cpu_baseline` (the --impl reference arm run in
+a fresh process, which also checks sampled outputs of every path against the
+exact product and times the reference's GPU build), `ref_gpu` (the reference's
+two GPU_FFNT calls against this library's drop-in and native products, at the
+workload's batch and at batch 1) and `nvbench` (the benchmark program
+gpu_ffnt_R_R_mult_benchmark built against this library and against the
+reference's, on the reference benchmark's axes).
 """
 from __future__ import annotations
 
