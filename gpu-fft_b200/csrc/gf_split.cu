@@ -163,6 +163,12 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
         long long hoff = 0; // 2^(w-1) (1 + 2^w + ... + 2^(w(k-2)))
         for (int i = 0; i + 1 < k; i++) hoff += 1LL << (w * i + w - 1);
         A.voff = hoff - A.K;
+        // V = x + voff over the input range (|x| < 2^input_bits, or 0 <= x <
+        // 2^input_bits for non-negative inputs)
+        const long long xlo = non_negative ? 0 : -(1LL << input_bits) + 1, xhi = (1LL << input_bits) - 1;
+        A.dig32 = (xlo + A.voff >= (long long)INT32_MIN && xhi + A.voff <= (long long)INT32_MAX && w * (k - 1) <= 30)
+                      ? 1
+                      : 0;
         unsigned long long S = 0; // sum_{l<k-1} 2^(w l)
         for (int i = 0; i + 1 < k; i++) S += 1ULL << (w * i);
         const unsigned long long K = (unsigned long long)A.K;
@@ -232,7 +238,10 @@ static int split_mul(const int32_t* a, const int32_t* b, int64_t* c, int n_power
                     GF_TRACE(tr, (double)wv * M * (2 * 2 * 4 + 2 * k * sizeof(cx<T>)), s,
                              "split_fwd0_col2<f32,L%d,k%d>", L0, k);
                     st = dispatch_int<1, SPLIT_TILE_MAXK>(k, [&]<int KK>() {
-                        return launch_k(split_fwd0_col2<SPLIT_COL_MAX, KK>, blocks, SPLIT_COL2_THREADS, 0, s, A);
+                        return A.dig32 ? launch_k(split_fwd0_col2<SPLIT_COL_MAX, KK, true>, blocks,
+                                                  SPLIT_COL2_THREADS, 0, s, A)
+                                       : launch_k(split_fwd0_col2<SPLIT_COL_MAX, KK, false>, blocks,
+                                                  SPLIT_COL2_THREADS, 0, s, A);
                     });
                 }
                 else

@@ -31,6 +31,8 @@
 // N <= 8192 runs all of it in one kernel (split_mid<true>).
 #pragma once
 
+#include <type_traits>
+
 #include "gf_pass.cuh"
 
 #include <algorithm>
@@ -73,6 +75,7 @@ template <typename T> struct SplitArgsT
     int uq, ur;        // K = 2^(w uq + ur): centring term joins groups s = l + uq, scaled 2^ur
     T scale;
     int w, k;
+    int dig32; // every V = x + voff fits an int32 and w (k - 1) <= 30: 32-bit digits
     long long W; // products per wave (stride of the workspace)
     long long batch;
     PassGeo geo;
@@ -488,7 +491,13 @@ __device__ __forceinline__ cx<float> shfl16(cx<float> v)
     return mk<float>(__shfl_xor_sync(0xffffffffu, v.x, 16), __shfl_xor_sync(0xffffffffu, v.y, 16));
 }
 
-template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5) split_fwd0_col2(const SplitArgs a)
+// The float value of a w-bit digit u (< 2^23) minus 2^(w-1): u placed in the
+// mantissa of 2^23, then one exact subtraction.
+__device__ __forceinline__ float digit_f(unsigned u, float bias) { return __int_as_float((int)(u | 0x4B000000u)) - bias; }
+
+// D32: every V = x + voff fits an int32 (a.dig32), digits in 32-bit arithmetic
+template <int L0, int K, bool D32>
+__global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4) split_fwd0_col2(const SplitArgs a)
 {
     pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L0, H = R / 2;
@@ -502,19 +511,33 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5
     const bool ok = bb < 2 * a.W; // the grid covers whole warps; every lane joins the exchange
     const long long op = bb >= a.W ? 1 : 0, p = ok ? bb - op * a.W : 0;
     const int32_t* src = (op == 0 ? a.a : a.b) + p * 2 * M + c;
-    long long v0[H], v1[H];
+    using V = typename std::conditional<D32, int, long long>::type;
+    V v0[H], v1[H];
     cx<float> tw[H];
 #pragma unroll
     for (int q = 0; q < H; q++)
     {
         const long long i = 2 * q + hb;
-        v0[q] = ok ? (long long)__ldg(src + i * C) + a.voff : 0;
-        v1[q] = ok ? (long long)__ldg(src + i * C + M) + a.voff : 0;
+        v0[q] = ok ? (V)((long long)__ldg(src + i * C) + a.voff) : 0;
+        v1[q] = ok ? (V)((long long)__ldg(src + i * C + M) + a.voff) : 0;
         tw[q] = ldg<float>(a.twist + c + i * C);
+    }
+    // the column's twiddles, the same for every limb: table[0 .. H/2) for the
+    // spans >= 2 and, for the span-1 stage, table[q] on half 1 (half 0 sends
+    // U unchanged, through a multiplication by 1)
+    cx<float> tws[H / 2], t1[H];
+    const float sg = hb ? -1.f : 1.f;
+#pragma unroll
+    for (int q = 0; q < H; q++)
+    {
+        const cx<float> t = ldg<float>(a.roots + q);
+        if (q < H / 2) tws[q] = t;
+        t1[q] = hb ? t : mk<float>(1.f, 0.f);
     }
     const int w = a.w;
     const long long mask = (1LL << w) - 1;
     const int half = 1 << (w - 1);
+    const float bias = 8388608.f + (float)half; // 2^23 + 2^(w-1)
     cx<float>* dst = a.spec + (op * K * a.W + p) * M + c;
 #pragma unroll
     for (int l = 0; l < K; l++)
@@ -523,20 +546,40 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5
 #pragma unroll
         for (int q = 0; q < H; q++)
         {
-            int d0, d1;
-            if (l < K - 1)
+            float f0, f1;
+            if constexpr (D32)
             {
-                d0 = (int)(v0[q] & mask) - half;
-                d1 = (int)(v1[q] & mask) - half;
-                v0[q] >>= w;
-                v1[q] >>= w;
+                // 32-bit digits: extract, then convert through the mantissa
+                if (l < K - 1)
+                {
+                    f0 = digit_f(((unsigned)v0[q] >> (w * l)) & (unsigned)mask, bias);
+                    f1 = digit_f(((unsigned)v1[q] >> (w * l)) & (unsigned)mask, bias);
+                }
+                else
+                {
+                    f0 = (float)(v0[q] >> (w * l));
+                    f1 = (float)(v1[q] >> (w * l));
+                }
             }
             else
             {
-                d0 = (int)v0[q];
-                d1 = (int)v1[q];
+                int d0, d1;
+                if (l < K - 1)
+                {
+                    d0 = (int)(v0[q] & mask) - half;
+                    d1 = (int)(v1[q] & mask) - half;
+                    v0[q] >>= w;
+                    v1[q] >>= w;
+                }
+                else
+                {
+                    d0 = (int)v0[q];
+                    d1 = (int)v1[q];
+                }
+                f0 = (float)d0;
+                f1 = (float)d1;
             }
-            x[q] = cmul<float>(mk<float>((float)d0, (float)d1), tw[q]);
+            x[q] = cmul<float>(mk<float>(f0, f1), tw[q]);
         }
         // stages s = 0 .. L0-2 (span h = 2^(L0-1-s) >= 2): rows q and q + h/2 of this lane
 #pragma unroll
@@ -545,16 +588,17 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5
             const int hh = 1 << (L0 - 2 - s);
 #pragma unroll
             for (int q = 0; q < H; q++)
-                if (!(q & hh)) ct_bfly<float>(x[q], x[q + hh], ldg<float>(a.roots + (q >> (L0 - 1 - s))));
+                if (!(q & hh)) ct_bfly<float>(x[q], x[q + hh], tws[q >> (L0 - 1 - s)]);
         }
-        // stage L0-1 (span 1): U = row 2q (half 0), V = row 2q+1 (half 1), table[q]
+        // stage L0-1 (span 1): U = row 2q (half 0), V = row 2q+1 (half 1),
+        // table[q]: half 1 sends V table[q], half 0 sends U; half 0 keeps the
+        // sum, half 1 the difference
 #pragma unroll
         for (int q = 0; q < H; q++)
         {
-            const cx<float> wt = ldg<float>(a.roots + q);
-            const cx<float> mine = hb ? cmul<float>(x[q], wt) : x[q]; // half 1 sends V w, half 0 sends U
+            const cx<float> mine = cmul<float>(x[q], t1[q]);
             const cx<float> other = shfl16(mine);
-            x[q] = hb ? csub<float>(other, mine) : cadd<float>(mine, other);
+            x[q] = __ffma2_rn(mine, make_float2(sg, sg), other);
         }
         if (ok)
         {
@@ -563,6 +607,23 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 5
             for (int q = 0; q < H; q++) d[(2 * q + hb) * C] = x[q];
         }
     }
+}
+
+// Round-to-nearest-even of |v| < 2^22 by one addition: v + 1.5 2^23 lands in
+// [2^23, 2^24), where the float spacing is 1, and the integer is the low bits
+// of the sum's encoding. Larger values are not certified (group_error), so
+// their integer does not matter.
+constexpr float RND_MAGIC = 12582912.0f; // 1.5 * 2^23
+constexpr int RND_MAGIC_BITS = 0x4B400000;
+
+// acc + i 2^sh (mod 2^64), sh uniform: one wide multiply-add below 2^31, one
+// add to the high word from 2^32 on
+__device__ __forceinline__ long long add_shifted(long long acc, int i, int sh)
+{
+    if (sh <= 30) return acc + (long long)i * (long long)(1 << sh);
+    if (sh >= 32)
+        return (long long)((unsigned long long)acc + ((unsigned long long)((unsigned)i << (sh - 32)) << 32));
+    return (long long)((unsigned long long)acc + ((unsigned long long)(long long)i << sh));
 }
 
 template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4) split_inv0_col2(const SplitArgs a)
@@ -585,10 +646,22 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4
         const cx<float> u = ldg<float>(a.untwist + c + (2 * q + hb) * C);
         un[q] = mk<float>(u.x * a.scale, u.y * a.scale); // scale folded in: exact, scale is 2^-m
     }
+    // the column's twiddles, the same for every group: table[0 .. H) for the
+    // span-1 stage (half 1 multiplies its difference; half 0 passes its sum on
+    // through a multiplication by 1) and table[0 .. H/2) for the others
+    cx<float> t1[H], tw[H / 2];
+    const float sg = hb ? -1.f : 1.f;
+#pragma unroll
+    for (int q = 0; q < H; q++)
+    {
+        const cx<float> t = ldg<float>(a.inv_roots + q);
+        if (q < H / 2) tw[q] = t;
+        t1[q] = hb ? t : mk<float>(1.f, 0.f);
+    }
     long long acc_lo[H], acc_hi[H];
 #pragma unroll
     for (int q = 0; q < H; q++) acc_lo[q] = acc_hi[q] = 0;
-    float err = 0.f;
+    float err = 0.f, big = 0.f;
     const cx<float>* src = a.group + p * M + c + hb * C;
     const long long gstride = a.W * M;
     cx<float> nx[H];
@@ -618,12 +691,13 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4
 #pragma unroll
             for (int q = 0; q < H; q++) nx[q] = __ldcs(src + (s + 1) * gstride + 2 * q * C);
         }
-        // stage L0-1 (span 1) first: U = row 2q (half 0), V = row 2q+1 (half 1), table[q]
+        // stage L0-1 (span 1) first: U = row 2q (half 0), V = row 2q+1 (half 1),
+        // table[q]: half 0 keeps U + V, half 1 takes (U - V) table[q]
 #pragma unroll
         for (int q = 0; q < H; q++)
         {
             const cx<float> other = shfl16(x[q]);
-            x[q] = hb ? cmul<float>(csub<float>(other, x[q]), ldg<float>(a.inv_roots + q)) : cadd<float>(x[q], other);
+            x[q] = cmul<float>(__ffma2_rn(x[q], make_float2(sg, sg), other), t1[q]);
         }
         // stages L0-2 .. 0 (span 2^(L0-1-st) >= 2), rows q and q + h/2 of this lane
 #pragma unroll
@@ -632,17 +706,19 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4
             const int hh = 1 << (L0 - 2 - st);
 #pragma unroll
             for (int q = 0; q < H; q++)
-                if (!(q & hh)) gs_bfly<float>(x[q], x[q + hh], ldg<float>(a.inv_roots + (q >> (L0 - 1 - st))));
+                if (!(q & hh)) gs_bfly<float>(x[q], x[q + hh], tw[q >> (L0 - 1 - st)]);
         }
         const int sh = a.w * s;
 #pragma unroll
         for (int q = 0; q < H; q++)
         {
             const cx<float> v = cmul<float>(x[q], un[q]);
-            const float rr = rintf(v.x), ri = rintf(v.y);
-            err = fmaxf(err, group_error(v, rr, ri));
-            acc_lo[q] += (long long)((unsigned long long)(long long)rr << sh);
-            acc_hi[q] += (long long)((unsigned long long)(long long)ri << sh);
+            const float tr = __fadd_rn(v.x, RND_MAGIC), ti = __fadd_rn(v.y, RND_MAGIC);
+            err = fmaxf(err, fmaxf(fabsf(__fsub_rn(v.x, __fsub_rn(tr, RND_MAGIC))),
+                                   fabsf(__fsub_rn(v.y, __fsub_rn(ti, RND_MAGIC)))));
+            big = fmaxf(big, fmaxf(fabsf(v.x), fabsf(v.y)));
+            acc_lo[q] = add_shifted(acc_lo[q], __float_as_int(tr) - RND_MAGIC_BITS, sh);
+            acc_hi[q] = add_shifted(acc_hi[q], __float_as_int(ti) - RND_MAGIC_BITS, sh);
         }
     }
     if (ok)
@@ -657,7 +733,8 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4
             __stcs(reinterpret_cast<long long*>(dst + i * C + M), acc_hi[q] + uu_term(a, j + M, 2 * M));
         }
     }
-    report_err(a.max_err, ok ? err : 0.f);
+    // values of 2^22 or more are not certified (group_error)
+    report_err(a.max_err, ok ? (big >= 4194304.0f ? 1.0f : err) : 0.f);
 }
 
 // FP32 columns of 8 points fit 128 registers: four CTAs (16 warps) per
