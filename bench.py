@@ -345,7 +345,7 @@ def ours_gpu_cases(gf, a64, b64, n_power, batch, args, dev, torch):
     cases = []
     for bt in (batch if b is None else b for b in REF_GPU_BATCHES):
         inout = torch.cat([a64[:bt].reshape(-1), b64[:bt].reshape(-1)]).double().to(dev)
-        temp = torch.empty(bt * h, dtype=torch.complex128, device=dev)
+        temp = torch.empty(2 * bt * h, dtype=torch.complex128, device=dev)  # spectra of 2 bt rows
         status = []
         ms_drop = events_ms(ffnt_product_calls(L.gpufft_ffnt_f64, (inout, temp), tables, n_power, bt, status),
                             args, torch, stream)
@@ -400,7 +400,7 @@ def reference_gpu_cases(args):
     cases = []
     for bt in (batch if b is None else b for b in REF_GPU_BATCHES):
         inout = torch.cat([a64[:bt].reshape(-1), b64[:bt].reshape(-1)]).double().to(dev)
-        temp = torch.empty(bt * h, dtype=torch.complex128, device=dev)
+        temp = torch.empty(2 * bt * h, dtype=torch.complex128, device=dev)  # spectra of 2 bt rows
         status = []
         ms = events_ms(ffnt_product_calls(R.ref_gpu_ffnt_f64, (inout, temp), tables, n_power, bt, status),
                        args, torch, stream)
