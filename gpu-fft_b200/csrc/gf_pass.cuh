@@ -536,8 +536,13 @@ __device__ __forceinline__ void col_pass_body(const PassArgs<T>& a, long long id
     }
 }
 
+// The column passes wait on global loads (one column's points and twiddles
+// per thread): eight-point double columns are compiled for eight CTAs per SM
+// (64 registers) so that more loads are in flight.
+template <typename T, int L> constexpr int col_min_blocks() { return (sizeof(T) == 8 && L <= 3) ? 8 : 1; }
+
 template <typename T, bool FWD, int L, int IK, int OK>
-__global__ void __launch_bounds__(COL_THREADS) col_pass_kernel(const PassArgs<T> a)
+__global__ void __launch_bounds__(COL_THREADS, col_min_blocks<T, L>()) col_pass_kernel(const PassArgs<T> a)
 {
     pdl_begin(); // before any global-memory access (programmatic launch)
     col_pass_body<T, FWD, L, IK, OK>(a, (long long)blockIdx.x * COL_THREADS + threadIdx.x);
