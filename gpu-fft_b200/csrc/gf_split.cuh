@@ -616,12 +616,13 @@ __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4) split_fwd0_col2(const S
 constexpr float RND_MAGIC = 12582912.0f; // 1.5 * 2^23
 constexpr int RND_MAGIC_BITS = 0x4B400000;
 
-// acc + i 2^sh (mod 2^64), sh uniform: one wide multiply-add below 2^31, one
-// add to the high word from 2^32 on
-__device__ __forceinline__ long long add_shifted(long long acc, int i, int sh)
+// acc + i 2^sh (mod 2^64) in the form MODE names (the caller picks it once
+// per group, sh being uniform): 0 one wide multiply-add (sh <= 30), 1 one add
+// to the high word (sh >= 32), 2 a 64-bit shift (sh = 31)
+template <int MODE> __device__ __forceinline__ long long add_shifted(long long acc, int i, int sh)
 {
-    if (sh <= 30) return acc + (long long)i * (long long)(1 << sh);
-    if (sh >= 32)
+    if constexpr (MODE == 0) return acc + (long long)i * (long long)(1 << sh);
+    if constexpr (MODE == 1)
         return (long long)((unsigned long long)acc + ((unsigned long long)((unsigned)i << (sh - 32)) << 32));
     return (long long)((unsigned long long)acc + ((unsigned long long)(long long)i << sh));
 }
@@ -709,17 +710,27 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4
                 if (!(q & hh)) gs_bfly<float>(x[q], x[q + hh], tw[q >> (L0 - 1 - st)]);
         }
         const int sh = a.w * s;
+        auto finish = [&](auto mode) {
+            constexpr int MODE = decltype(mode)::value;
 #pragma unroll
-        for (int q = 0; q < H; q++)
-        {
-            const cx<float> v = cmul<float>(x[q], un[q]);
-            const float tr = __fadd_rn(v.x, RND_MAGIC), ti = __fadd_rn(v.y, RND_MAGIC);
-            err = fmaxf(err, fmaxf(fabsf(__fsub_rn(v.x, __fsub_rn(tr, RND_MAGIC))),
-                                   fabsf(__fsub_rn(v.y, __fsub_rn(ti, RND_MAGIC)))));
-            big = fmaxf(big, fmaxf(fabsf(v.x), fabsf(v.y)));
-            acc_lo[q] = add_shifted(acc_lo[q], __float_as_int(tr) - RND_MAGIC_BITS, sh);
-            acc_hi[q] = add_shifted(acc_hi[q], __float_as_int(ti) - RND_MAGIC_BITS, sh);
-        }
+            for (int q = 0; q < H; q++)
+            {
+                const cx<float> v = cmul<float>(x[q], un[q]);
+                const float tr = __fadd_rn(v.x, RND_MAGIC), ti = __fadd_rn(v.y, RND_MAGIC);
+                err = fmaxf(err, fmaxf(fabsf(__fsub_rn(v.x, __fsub_rn(tr, RND_MAGIC))),
+                                       fabsf(__fsub_rn(v.y, __fsub_rn(ti, RND_MAGIC)))));
+                big = fmaxf(big, fmaxf(fabsf(v.x), fabsf(v.y)));
+                acc_lo[q] = add_shifted<MODE>(acc_lo[q], __float_as_int(tr) - RND_MAGIC_BITS, sh);
+                acc_hi[q] = add_shifted<MODE>(acc_hi[q], __float_as_int(ti) - RND_MAGIC_BITS, sh);
+            }
+        };
+        // one uniform branch per group
+        if (sh <= 30)
+            finish(std::integral_constant<int, 0>{});
+        else if (sh >= 32)
+            finish(std::integral_constant<int, 1>{});
+        else
+            finish(std::integral_constant<int, 2>{});
     }
     if (ok)
     {
