@@ -402,6 +402,9 @@ template <int L> __global__ void __launch_bounds__(NTHR) split_inv0(const SplitA
 // identical.
 // --------------------------------------------------------------------------
 constexpr int SPLIT_COL_MAX = 4;
+// log2 of the tile kernel's tile (gf_split_tile.cuh); its column passes run the
+// first / last m - SPLIT_TILE_LT stages
+constexpr int SPLIT_TILE_LT = 11;
 constexpr int SPLIT_COL_THREADS = 128;
 
 // One thread per column of one operand of one product: the column's 2 x 2^L0
@@ -501,8 +504,10 @@ __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4) split_fwd0_col2(const S
 {
     pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L0, H = R / 2;
-    const int m = a.geo.m;
-    const long long M = 1LL << m, C = M >> L0;
+    // the tile path's column passes only: m = L0 + SPLIT_TILE_LT, all
+    // column offsets compile-time
+    constexpr int m = L0 + SPLIT_TILE_LT;
+    constexpr long long M = 1LL << m, C = M >> L0;
     const long long idx = (long long)blockIdx.x * SPLIT_COL2_THREADS + threadIdx.x;
     const int hb = (int)((idx >> 4) & 1);
     const long long col = ((idx >> 5) << 4) + (idx & 15); // column over all (operand, product)
@@ -631,8 +636,10 @@ template <int L0, int K> __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4
 {
     pdl_begin(); // before any global-memory access (programmatic launch)
     constexpr int R = 1 << L0, H = R / 2;
-    const int m = a.geo.m;
-    const long long M = 1LL << m, C = M >> L0;
+    // the tile path's column passes only: m = L0 + SPLIT_TILE_LT, all
+    // column offsets compile-time
+    constexpr int m = L0 + SPLIT_TILE_LT;
+    constexpr long long M = 1LL << m, C = M >> L0;
     const long long idx = (long long)blockIdx.x * SPLIT_COL2_THREADS + threadIdx.x;
     const int hb = (int)((idx >> 4) & 1);
     const long long col = ((idx >> 5) << 4) + (idx & 15);
@@ -906,7 +913,7 @@ template <int L, bool SINGLE, int K> static int launch_mid_k(const SplitArgs& a,
 // The split product's contiguous stages of every limb and limb group on
 // 2^SPLIT_TILE_LT-point tiles held in shared memory (gf_split_tile.cuh), for
 // up to SPLIT_TILE_MAXK limbs; compiled in gf_split_tile.cu.
-constexpr int SPLIT_TILE_LT = 11;
+// (SPLIT_TILE_LT is defined with the column kernels above.)
 constexpr int SPLIT_TILE_MAXK = 5;
 int launch_split_tile(int k, const SplitArgs& a, long long tiles, cudaStream_t s);
 
