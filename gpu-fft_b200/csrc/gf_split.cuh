@@ -523,8 +523,11 @@ __global__ void __launch_bounds__(SPLIT_COL2_THREADS, 4) split_fwd0_col2(const S
     for (int q = 0; q < H; q++)
     {
         const long long i = 2 * q + hb;
-        v0[q] = ok ? (V)((long long)__ldg(src + i * C) + a.voff) : 0;
-        v1[q] = ok ? (V)((long long)__ldg(src + i * C + M) + a.voff) : 0;
+        // out-of-range lanes read product 0 (p = 0 keeps src inside the inputs):
+        // their results are never stored, and their exchange partner (lane ^ 16,
+        // the same column) is out of range too
+        v0[q] = (V)((long long)__ldg(src + i * C) + a.voff);
+        v1[q] = (V)((long long)__ldg(src + i * C + M) + a.voff);
         tw[q] = ldg<float>(a.twist + c + i * C);
     }
     // the column's twiddles, the same for every limb: table[0 .. H/2) for the
